@@ -1,0 +1,182 @@
+/* pgb.h -- C ABI of the B200 graph beam search (ParlayANN search API as a drop-in).
+ *
+ * Plain C: pointers, sizes, status codes. No exceptions cross this boundary and no
+ * call exits the process (the reference's CHECK_CUDA exits, cuda/comun.h:57-65; here
+ * every failure is a pgb_status plus a message from pgb_last_error()).
+ *
+ * What each group replaces in the reference (paths inside the reference project):
+ *   pgb_index_*     <- subirVectores / subirGrafo / subirHnsw + the readers
+ *                      (cuda/datos_gpu.cu:61-122, cuda/busqueda_hnsw.cu:462-530,
+ *                      cuda/lectores.cpp:113-187, cuda/hnsw_lector.cpp:336-419)
+ *   pgb_searcher_*  <- BuscadorGPU / BuscadorHnsw preparar, lanzar, liberar
+ *                      (cuda/busqueda.cuh:36-61, cuda/busqueda.cu:525-594,
+ *                      cuda/hnsw.h:65-86, cuda/busqueda_hnsw.cu:551-645)
+ *   pgb_query_params <- ConfigBusqueda (cuda/busqueda.cuh:6-11) extended to ParlayANN's
+ *                      QueryParams{k, beamSize, cut, limit, degree_limit}
+ *   pgb_query_stats <- compDev / banderasDev (cuda/busqueda.cuh:43-46) + expansions
+ *   pgb_recall      <- calcularRecall (cuda/evaluacion.cpp:184-208)
+ *   pgb_batch_*, pgb_server_* have no counterpart in the reference: the batched
+ *                      persistent form and the serving loop built on top of the plain
+ *                      warp-per-query search, returning identical neighbours.
+ *   pgb_build_*     <- ParlayANN's CPU graph builders (absent from the reference; it
+ *                      clones them at run time, cpu_baseline/setup.sh:45-52).
+ *
+ * Memory: an index owns its device copy of vectors and graph and is read-only after
+ * creation. A searcher / batch owns its scratch; outputs are caller-owned device
+ * buffers (pgb_searcher_search) or host buffers (pgb_searcher_search_host).
+ * Threading: one index may be searched from several host threads, each with its own
+ * searcher and stream.
+ */
+#ifndef PGB_H_
+#define PGB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pgb_status {
+    PGB_OK = 0,
+    PGB_ERR_BAD_ARG = 1,     /* invalid argument or size beyond a supported maximum */
+    PGB_ERR_OOM = 2,         /* device or pinned allocation failed                  */
+    PGB_ERR_CUDA = 3,        /* a CUDA runtime call failed                          */
+    PGB_ERR_OVERFLOW = 4,    /* a capacity counter would wrap (reuse limit reached) */
+    PGB_ERR_IO = 5,          /* file could not be opened / read / written           */
+    PGB_ERR_FORMAT = 6,      /* file or arrays violate the format                   */
+    PGB_ERR_BUSY = 7,        /* server: no free slot or memory for the request      */
+    PGB_ERR_TIMEOUT = 8,     /* a bounded wait gave up                              */
+    PGB_ERR_NOT_FOUND = 9    /* server: unknown ticket                              */
+} pgb_status;
+
+/* element type of the vectors */
+typedef enum pgb_elem { PGB_INT8 = 0, PGB_UINT8 = 1 } pgb_elem;
+
+#define PGB_NO_NEIGHBOR 0xFFFFFFFFu /* output padding id (reference SIN_VECINO)      */
+#define PGB_FLAG_OVERFLOW 1         /* visited table past half capacity (BANDERA_DESBORDE) */
+#define PGB_FLAG_SHORT 2            /* frontier ended with fewer than k entries       */
+#define PGB_MAX_DEGREE 256          /* rows wider than this are rejected              */
+#define PGB_MAX_BEAM 1024           /* largest beam size (Ls) accepted                */
+#define PGB_MAX_K 1024              /* largest k accepted                             */
+#define PGB_MAX_DIM 128             /* vectors are stored as 128-byte rows            */
+#define PGB_MAX_HNSW_ENTRIES 8      /* reference MAX_ENTRADAS_HNSW (cuda/hnsw.h:9)    */
+
+typedef struct pgb_query_params {
+    uint32_t k;                /* neighbours returned                                  */
+    uint32_t beam_size;        /* Ls: frontier width (HNSW: layer-0 ef)                */
+    double cut;                /* frontier cut factor (flat graphs; reference 1.35)    */
+    int64_t limit;             /* max expansions ("visit"); <= 0 means n               */
+    uint32_t degree_limit;     /* first degree_limit row entries used; 0 = max degree  */
+    uint32_t exclude_query_id; /* 1: skip neighbour id == query index, as ParlayANN's
+                                  wrapper does with `a == p.id()` (flat graphs only)   */
+    uint32_t query_id_base;    /* query index of the first query of the call           */
+    uint32_t reserved;
+} pgb_query_params;
+
+typedef struct pgb_query_stats {
+    int32_t dist_comps;  /* distance computations, counted as the reference does */
+    int32_t expansions;  /* frontier nodes expanded                              */
+    int32_t flags;       /* PGB_FLAG_* bits                                       */
+    int32_t reserved;
+} pgb_query_stats;
+
+typedef struct pgb_index_info {
+    uint32_t n_points;
+    uint32_t dim;
+    uint32_t elem;          /* pgb_elem                                   */
+    uint32_t is_hnsw;
+    uint32_t max_degree;    /* flat: G; HNSW: level-0 degree G0            */
+    uint32_t upper_degree;  /* HNSW: upper-level degree GA; flat: 0        */
+    uint32_t top_level;     /* HNSW only                                  */
+    uint32_t n_entries;     /* HNSW only                                  */
+    uint64_t device_bytes;  /* vectors + graph resident on the device     */
+} pgb_index_info;
+
+typedef struct pgb_index pgb_index;
+typedef struct pgb_searcher pgb_searcher;
+typedef struct pgb_batch pgb_batch;
+typedef struct pgb_server pgb_server;
+
+/* ---- errors ---------------------------------------------------------------- */
+const char* pgb_status_string(pgb_status s);
+/* message of the last failing call on this host thread ("" if none) */
+const char* pgb_last_error(void);
+/* 1 if a CUDA device of compute capability 10.x is visible, else 0 */
+int pgb_device_available(void);
+
+/* ---- index ------------------------------------------------------------------- */
+/* Flat fixed-degree graph (Vamana/DiskANN, HCNNG, PyNNDescent) from host arrays.
+ * vectors: n rows of dim bytes (int8 or uint8, packed). Graph in ParlayANN's layout:
+ * degrees[n], edges = all rows concatenated (sum(degrees) ids < n). */
+pgb_status pgb_index_create_flat(int device, const void* vectors, uint32_t n, uint32_t dim,
+                                 pgb_elem elem, const uint32_t* degrees,
+                                 const uint32_t* edges, pgb_index** out);
+/* HNSW from host arrays in the order of the ParlayANN HNSW v3 file (cuda/hnsw.h:11-16):
+ * per node i (0..n_nodes-1) its top level levels[i] and stored point node_point[i];
+ * list_sizes / ids: the neighbour lists of node 0 levels 0..levels[0], node 1, ... */
+pgb_status pgb_index_create_hnsw(int device, const void* vectors, uint32_t n_points,
+                                 uint32_t dim, pgb_elem elem, uint32_t n_nodes,
+                                 const uint32_t* levels, const uint32_t* node_point,
+                                 const uint32_t* list_sizes, const uint32_t* ids,
+                                 const uint32_t* entries, uint32_t n_entries,
+                                 pgb_index** out);
+/* From files: .i8bin / .u8bin vectors ([n u32][dim u32][n*dim bytes]), a ParlayANN
+ * graph ([n u32][maxdeg u32][deg n*u32][edges]) or HNSW v3 model. */
+pgb_status pgb_index_load_flat(int device, const char* vectors_path, pgb_elem elem,
+                               const char* graph_path, pgb_index** out);
+pgb_status pgb_index_load_hnsw(int device, const char* vectors_path, pgb_elem elem,
+                               const char* hnsw_path, pgb_index** out);
+pgb_status pgb_index_get_info(const pgb_index* index, pgb_index_info* out);
+pgb_status pgb_index_destroy(pgb_index* index);
+
+/* ---- plain warp-per-query search (the drop-in) ------------------------------------ */
+/* preparar: scratch for up to max_queries queries with these params. */
+pgb_status pgb_searcher_create(pgb_index* index, uint32_t max_queries,
+                               const pgb_query_params* params, pgb_searcher** out);
+/* lanzar: asynchronous on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * queries: device pointer, nq rows of index dim bytes, `query_stride` bytes apart.
+ * Outputs (device): ids[nq*k], dists[nq*k], stats[nq] (stats may be NULL). Rows of
+ * queries that end with fewer than k entries are padded with PGB_NO_NEIGHBOR/INT32_MAX. */
+pgb_status pgb_searcher_search(pgb_searcher* s, const void* queries, uint32_t nq,
+                               uint32_t query_stride, uint32_t* ids, int32_t* dists,
+                               pgb_query_stats* stats, void* stream);
+/* Same search from and to HOST memory, synchronous: copies the queries in, searches,
+ * copies ids / dists / stats (stats may be NULL) out. */
+pgb_status pgb_searcher_search_host(pgb_searcher* s, const void* queries, uint32_t nq,
+                                    uint32_t query_stride, uint32_t* ids, int32_t* dists,
+                                    pgb_query_stats* stats);
+/* liberar */
+pgb_status pgb_searcher_destroy(pgb_searcher* s);
+
+/* ---- evaluation ---------------------------------------------------------------- */
+/* recall@k with distance ties (big-ann-benchmarks compute_recall_with_distance_ties). */
+double pgb_recall(const uint32_t* gt_ids, const float* gt_dists, uint32_t nq, uint32_t gt_k,
+                  const uint32_t* ids, uint32_t k);
+
+/* ---- graph builders (CPU, deterministic for a seed) ---------------------------------
+ * vectors: n packed rows of dim bytes. nthreads <= 0: all host threads.
+ * Outputs: degrees[n] and a padded n x slots adjacency (PGB_NO_NEIGHBOR padding),
+ * slots = R (Vamana), trees*mst_deg (HCNNG), K (NN-descent). */
+pgb_status pgb_build_vamana(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
+                            uint32_t R, uint32_t L, float alpha, int passes, uint64_t seed,
+                            int nthreads, uint32_t* degrees, uint32_t* adjacency);
+pgb_status pgb_build_hcnng(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
+                           uint32_t trees, uint32_t leaf, uint32_t mst_deg, uint64_t seed,
+                           int nthreads, uint32_t* degrees, uint32_t* adjacency);
+pgb_status pgb_build_nndescent(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
+                               uint32_t K, uint32_t init_trees, uint32_t leaf, float alpha,
+                               float delta, uint32_t max_iters, uint64_t seed, int nthreads,
+                               uint32_t* degrees, uint32_t* adjacency);
+/* HNSW written straight to an HNSW v3 model file. */
+pgb_status pgb_build_hnsw(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
+                          uint32_t M, uint32_t ef_construction, float ml, float alpha,
+                          uint64_t seed, int nthreads, const char* path);
+/* ParlayANN graph file from a padded adjacency (row i: degrees[i] ids, stride slots). */
+pgb_status pgb_write_graph(const char* path, uint32_t n, uint32_t slots,
+                           const uint32_t* degrees, const uint32_t* adjacency);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PGB_H_ */

@@ -1,0 +1,32 @@
+// builders.h -- CPU graph builders (see builders.cpp).
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "host_common.h"
+
+namespace pgb {
+
+// HNSW built in memory: one row of capacity (2M at level 0, M above) per (node, level).
+struct HnswBuilt {
+    uint32_t n = 0, M = 0;
+    std::vector<uint32_t> level;
+    std::vector<uint64_t> first;    // index of node i's level-0 row
+    std::vector<uint32_t> rows;     // row storage
+    std::vector<uint32_t> sizes;    // per (node, level)
+    std::vector<uint64_t> row_off;  // per (node, level): offset in rows
+    uint32_t entry = 0;
+};
+
+int build_vamana(const HostVectors& V, uint32_t R, uint32_t L, float alpha, int passes,
+                 uint64_t seed, int nthreads, uint32_t* out_deg, uint32_t* out_adj);
+int build_hcnng(const HostVectors& V, uint32_t trees, uint32_t leaf, uint32_t mst_deg,
+                uint64_t seed, int nthreads, uint32_t* out_deg, uint32_t* out_adj);
+int build_nndescent(const HostVectors& V, uint32_t K, uint32_t init_trees, uint32_t leaf,
+                    float alpha, float delta, uint32_t max_iters, uint64_t seed, int nthreads,
+                    uint32_t* out_deg, uint32_t* out_adj);
+int build_hnsw(const HostVectors& V, uint32_t M, uint32_t efc, float ml, float alpha,
+               uint64_t seed, int nthreads, HnswBuilt& H);
+
+}  // namespace pgb

@@ -1,0 +1,117 @@
+// device_common.cuh -- device primitives shared by the flat and HNSW search kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pgb {
+
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr uint32_t kEmptyId = 0xFFFFFFFFu;      // row padding / empty table slot
+constexpr uint64_t kEmptyKey = ~0ull;           // sentinel (dist, id) key, sorts last
+constexpr int kRowBytes = 128;                  // every vector row occupies 128 bytes
+
+// parlaylib hash64_2: filter slots must land where ParlayANN's land
+// (reference cuda/utiles_gpu.cuh:12-17)
+__device__ __forceinline__ uint64_t hash64_2(uint64_t x) {
+    x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+    x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+// parlaylib hash64; HNSW marks its entry points with it (cuda/utiles_gpu.cuh:21-31)
+__device__ __forceinline__ uint64_t hash64(uint64_t u) {
+    uint64_t v = u * 3935559000370003845ull + 2691343689449507681ull;
+    v ^= v >> 21;
+    v ^= v << 37;
+    v ^= v >> 4;
+    v *= 4768777513237032717ull;
+    v ^= v << 20;
+    v ^= v >> 41;
+    v ^= v << 5;
+    return v;
+}
+
+// (dist, id) packed so that unsigned order == ParlayANN's pair order
+// (distances are >= 0 and below 2^24 for 128 bytes of 8-bit values)
+__device__ __forceinline__ uint64_t pack_key(int32_t d, uint32_t id) {
+    return ((uint64_t)(uint32_t)d << 32) | id;
+}
+__device__ __forceinline__ int32_t key_dist(uint64_t k) { return (int32_t)(k >> 32); }
+__device__ __forceinline__ uint32_t key_id(uint64_t k) { return (uint32_t)k; }
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+__device__ __forceinline__ uint32_t lanemask_gt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_gt;" : "=r"(m));
+    return m;
+}
+
+// 16 bytes of one 128-byte row: dot(p, p) - 2 dot(p, q) over those bytes.
+// Summed over the 8 lanes of a row this plus ||q||^2 is ||q - p||^2 exactly
+// (the reference computes the same integer with a stored norm, cuda/distancia.cuh:43-58;
+// here ||p||^2 comes from the row itself, so no norm array is gathered).
+template <bool Signed>
+__device__ __forceinline__ int32_t partial_l2(const int4 p, const int4 q) {
+    int32_t pp, pq;
+    if (Signed) {
+        pp = __dp4a(p.x, p.x, 0);
+        pp = __dp4a(p.y, p.y, pp);
+        pp = __dp4a(p.z, p.z, pp);
+        pp = __dp4a(p.w, p.w, pp);
+        pq = __dp4a(p.x, q.x, 0);
+        pq = __dp4a(p.y, q.y, pq);
+        pq = __dp4a(p.z, q.z, pq);
+        pq = __dp4a(p.w, q.w, pq);
+    } else {
+        pp = (int32_t)__dp4a((uint32_t)p.x, (uint32_t)p.x, 0u);
+        pp = (int32_t)__dp4a((uint32_t)p.y, (uint32_t)p.y, (uint32_t)pp);
+        pp = (int32_t)__dp4a((uint32_t)p.z, (uint32_t)p.z, (uint32_t)pp);
+        pp = (int32_t)__dp4a((uint32_t)p.w, (uint32_t)p.w, (uint32_t)pp);
+        pq = (int32_t)__dp4a((uint32_t)p.x, (uint32_t)q.x, 0u);
+        pq = (int32_t)__dp4a((uint32_t)p.y, (uint32_t)q.y, (uint32_t)pq);
+        pq = (int32_t)__dp4a((uint32_t)p.z, (uint32_t)q.z, (uint32_t)pq);
+        pq = (int32_t)__dp4a((uint32_t)p.w, (uint32_t)q.w, (uint32_t)pq);
+    }
+    return pp - 2 * pq;
+}
+
+template <bool Signed>
+__device__ __forceinline__ int32_t partial_sq(const int4 q) {
+    if (Signed) {
+        int32_t s = __dp4a(q.x, q.x, 0);
+        s = __dp4a(q.y, q.y, s);
+        s = __dp4a(q.z, q.z, s);
+        return __dp4a(q.w, q.w, s);
+    } else {
+        uint32_t s = __dp4a((uint32_t)q.x, (uint32_t)q.x, 0u);
+        s = __dp4a((uint32_t)q.y, (uint32_t)q.y, s);
+        s = __dp4a((uint32_t)q.z, (uint32_t)q.z, s);
+        return (int32_t)__dp4a((uint32_t)q.w, (uint32_t)q.w, s);
+    }
+}
+
+// read-only 16-byte load through the non-coherent path
+__device__ __forceinline__ int4 ldg16(const void* p) {
+    return __ldg(reinterpret_cast<const int4*>(p));
+}
+
+// Loads a query of `dim` bytes (any alignment) into a zero-padded 128-byte row in
+// shared memory: lane l fills bytes 4l..4l+3.
+__device__ __forceinline__ void load_query_row(const uint8_t* src, uint32_t dim, int lane,
+                                               uint32_t* dst_words) {
+    uint32_t w = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+        uint32_t i = 4u * lane + b;
+        uint32_t v = (i < dim) ? (uint32_t)src[i] : 0u;
+        w |= v << (8 * b);
+    }
+    dst_words[lane] = w;
+}
+
+}  // namespace pgb

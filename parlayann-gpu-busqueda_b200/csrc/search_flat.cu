@@ -1,0 +1,141 @@
+// search_flat.cu -- the two schedules of the flat-graph beam search.
+//
+// plain   : the drop-in. Persistent grid, warp w takes queries w, w+W, ... (the
+//           reference's schedule, cuda/busqueda.cu:151-152), one Ls and k per launch.
+// batched : persistent grid whose warps pull queries from a device counter over a
+//           longest-beam-first order, each query with its own Ls and k; tables sized
+//           for the batch's largest Ls. Same per-query code, identical neighbours.
+#include <algorithm>
+#include <cstdio>
+
+#include "errors.h"
+#include "search_flat.cuh"
+#include "search_plan.h"
+
+namespace pgb {
+
+template <int CH, bool Signed, bool SFILT>
+__global__ void __launch_bounds__(256) flat_plain_kernel(FlatArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t gw = blockIdx.x * wpb + w;
+    const uint32_t total = gridDim.x * wpb;
+    unsigned char* wmem = smem + (size_t)w * A.L.bytes;
+    uint32_t* gf = A.gfilter ? A.gfilter + (size_t)gw * A.gfilter_words : nullptr;
+    uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
+    for (uint32_t q = gw; q < A.nq; q += total)
+        flat_query<CH, Signed, SFILT>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
+}
+
+template <int CH, bool Signed, bool SFILT>
+__global__ void __launch_bounds__(256) flat_batched_kernel(FlatArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t gw = blockIdx.x * wpb + w;
+    unsigned char* wmem = smem + (size_t)w * A.L.bytes;
+    uint32_t* gf = A.gfilter ? A.gfilter + (size_t)gw * A.gfilter_words : nullptr;
+    uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
+    for (;;) {
+        uint32_t slot = 0;
+        if (lane == 0) slot = atomicAdd(A.queue, 1u);
+        slot = __shfl_sync(kFull, slot, 0);
+        if (slot >= A.nq) break;
+        const uint32_t q = A.order[slot];
+        flat_query<CH, Signed, SFILT>(A, wmem, gf, gv, q, A.ls_arr[q], A.k_arr[q], lane);
+    }
+}
+
+namespace {
+
+using KernelFn = void (*)(FlatArgs);
+
+template <int CH, bool Signed, bool SFILT>
+KernelFn pick_kernel(bool batched) {
+    return batched ? flat_batched_kernel<CH, Signed, SFILT> : flat_plain_kernel<CH, Signed, SFILT>;
+}
+
+template <int CH>
+KernelFn pick_ch(bool batched, bool is_signed, bool sfilt) {
+    if (is_signed) return sfilt ? pick_kernel<CH, true, true>(batched) : pick_kernel<CH, true, false>(batched);
+    return sfilt ? pick_kernel<CH, false, true>(batched) : pick_kernel<CH, false, false>(batched);
+}
+
+KernelFn pick(int ch, bool batched, bool is_signed, bool sfilt) {
+    switch (ch) {
+        case 1: return pick_ch<1>(batched, is_signed, sfilt);
+        case 2: return pick_ch<2>(batched, is_signed, sfilt);
+        case 3: return pick_ch<3>(batched, is_signed, sfilt);
+        case 4: return pick_ch<4>(batched, is_signed, sfilt);
+        default: return pick_ch<8>(batched, is_signed, sfilt);
+    }
+}
+
+}  // namespace
+
+int flat_chunks_for(uint32_t gs) {
+    int ch = (int)((gs + 31) / 32);
+    return ch <= 4 ? ch : 8;
+}
+
+pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
+    P = FlatPlan{};
+    P.ch = flat_chunks_for(rq.deg_lim);
+    P.batched = rq.batched;
+    P.is_signed = rq.is_signed;
+    const uint32_t ls = rq.max_ls;
+    const uint32_t fwords = 1u << flat_filter_bits(ls);
+    const uint32_t vwords = flat_visited_cap(ls);
+    P.sfilt = rq.force_filter_placement ? rq.filter_in_shared
+                                        : (4ull * fwords <= rq.filter_smem_limit);
+    P.svis = rq.force_visited_placement ? rq.visited_in_shared
+                                        : (4ull * vwords <= rq.visited_smem_limit);
+    const uint32_t ls_cap = (ls + 7u) & ~7u;
+    P.L = make_flat_layout(ls_cap, 32u * P.ch, P.sfilt ? fwords : 0u, P.svis ? vwords : 0u);
+    P.gfilter_words = P.sfilt ? 0u : fwords;
+    P.gvisited_words = P.svis ? 0u : vwords;
+    P.kernel = (void*)pick(P.ch, P.batched, P.is_signed, P.sfilt);
+
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(PGB_ERR_CUDA, "cudaGetDevice failed");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
+        return fail(PGB_ERR_CUDA, "cudaGetDeviceProperties failed");
+    const size_t smem_cap = prop.sharedMemPerBlockOptin;
+    int wpb = rq.warps_per_block > 0 ? rq.warps_per_block : 4;
+    while (wpb > 1 && (size_t)wpb * P.L.bytes > smem_cap) wpb >>= 1;
+    if ((size_t)wpb * P.L.bytes > smem_cap)
+        return fail(PGB_ERR_BAD_ARG, "beam too wide for shared memory with this placement");
+    P.warps_per_block = wpb;
+    P.smem_bytes = (size_t)wpb * P.L.bytes;
+    cudaError_t e = cudaFuncSetAttribute(P.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)P.smem_bytes);
+    if (e != cudaSuccess)
+        return fail(PGB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    int bps = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, P.kernel, wpb * 32, P.smem_bytes);
+    if (e != cudaSuccess || bps < 1)
+        return fail(PGB_ERR_CUDA, "kernel does not fit on a multiprocessor");
+    if (rq.max_blocks_per_sm > 0) bps = std::min(bps, rq.max_blocks_per_sm);
+    P.blocks_per_sm = bps;
+    P.blocks = bps * prop.multiProcessorCount;
+    P.total_warps = (uint64_t)P.blocks * wpb;
+    return PGB_OK;
+}
+
+pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
+    A.L = P.L;
+    A.gfilter_words = P.gfilter_words;
+    A.gvisited_words = P.gvisited_words;
+    void* args[] = {&A};
+    cudaError_t e = cudaLaunchKernel(P.kernel, dim3(P.blocks), dim3(P.warps_per_block * 32),
+                                     args, P.smem_bytes, stream);
+    if (e != cudaSuccess)
+        return fail(PGB_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
+    return PGB_OK;
+}
+
+}  // namespace pgb

@@ -1,0 +1,552 @@
+// search_flat.cuh -- one query of ParlayANN beam_search over a fixed-degree graph,
+// executed by one warp. Shared by the plain kernel and the batched persistent kernel,
+// so both return bit-identical neighbours.
+//
+// Semantics (same integers, same order as the reference kernel, cuda/busqueda.cu:151-499):
+//   F = {(d(q, start), start)}, comps = 1; lossy filter H[2^bits] cleared per query
+//   while an unvisited entry of F exists and expansions < limit:
+//     u = first unvisited entry; mark visited; expansions++ (overflow rule :205-208)
+//     for the first degree_limit row entries a, in row order: skip a == query index
+//       (when requested) and a seen by the lossy filter (slot hash64_2(a) & mask);
+//       every survivor costs one distance (comps++)
+//     candidates: d < cutoff (INT_MAX while |F| < Ls, else F.back().d), sorted by (d, id)
+//     F = first Ls of multiset set_union(F, candidates); cut at
+//       upper_bound(F, (id 0, float(cut * F[k].d))) under (float dist, id) order
+//   output: first k entries of F (padded), comps, expansions, flags
+//
+// Layout per warp (shared memory): query row, frontier keys + visited bytes, candidate
+// scratch, and -- when they fit -- the lossy filter and the exact visited table.
+#pragma once
+
+#include <climits>
+
+#include "../../include/pgb.h"
+#include "device_common.cuh"
+
+namespace pgb {
+
+__host__ __device__ inline int ceil_log2_u64(uint64_t x) {
+    int b = 0;
+    while ((1ull << b) < x) b++;
+    return b;
+}
+__host__ __device__ inline uint32_t next_pow2_u32(uint32_t x) {
+    uint32_t p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+// lossy filter size, a semantic parameter (reference cuda/busqueda.cu:536-538)
+__host__ __device__ inline int flat_filter_bits(uint32_t Ls) {
+    int b = ceil_log2_u64((uint64_t)Ls * Ls) - 2;
+    return b > 10 ? b : 10;
+}
+// exact visited-table capacity and the expansion count that raises the overflow flag
+// (reference cuda/busqueda.cu:540 and :205-208)
+__host__ __device__ inline uint32_t flat_visited_cap(uint32_t Ls) {
+    return next_pow2_u32(8u * Ls + 128u);
+}
+
+struct FlatLayout {
+    uint32_t ls_cap;         // frontier capacity (>= largest Ls served)
+    uint32_t gs;             // adjacency row stride, multiple of 32 (>= degree limit)
+    uint32_t filter_words;   // lossy filter words kept in shared memory (0: global)
+    uint32_t visited_words;  // visited-table words in shared memory (0: global)
+    uint32_t off_fkey, off_fvis, off_a, off_b, off_c, off_filter, off_visited, bytes;
+};
+
+__host__ __device__ inline uint32_t round16(uint32_t x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ inline FlatLayout make_flat_layout(uint32_t ls_cap, uint32_t gs,
+                                                       uint32_t filter_words,
+                                                       uint32_t visited_words) {
+    FlatLayout L;
+    L.ls_cap = ls_cap;
+    L.gs = gs;
+    L.filter_words = filter_words;
+    L.visited_words = visited_words;
+    uint32_t o = kRowBytes;  // query row at offset 0
+    L.off_fkey = o;
+    o += 8u * ls_cap;
+    L.off_fvis = o;
+    o = round16(o + ls_cap);
+    L.off_a = o;  // pending ids + distances, later entering keys
+    o += 8u * gs;
+    L.off_b = o;  // candidate keys
+    o += 8u * gs;
+    L.off_c = o;  // entering positions + visited bytes
+    o = round16(o + 5u * gs);
+    L.off_filter = o;
+    o += 4u * filter_words;
+    L.off_visited = o;
+    o += 4u * visited_words;
+    L.bytes = round16(o);
+    return L;
+}
+
+struct FlatArgs {
+    const uint8_t* rows;   // n x 128-byte vector rows
+    const uint32_t* adj;   // n x gs neighbour ids, padded with kEmptyId
+    uint32_t n, gs, deg_lim, dim, start;
+    const uint8_t* queries;
+    uint32_t nq, qstride;
+    double cut;
+    int64_t limit;         // resolved: > 0
+    uint32_t excl, qbase;
+    uint32_t Ls, k;                 // uniform values (plain kernel)
+    const uint32_t* ls_arr;         // per-query Ls (batched), indexed by query
+    const uint32_t* k_arr;          // per-query k (batched)
+    const uint32_t* order;          // batched: processing order of the queries
+    uint32_t out_stride;            // output row stride (>= k)
+    uint32_t* ids;
+    int32_t* dists;
+    pgb_query_stats* stats;
+    FlatLayout L;
+    uint32_t* gfilter;              // per-warp global filters when not in shared memory
+    uint32_t gfilter_words;
+    uint32_t* gvisited;             // per-warp global visited tables when not in shared
+    uint32_t gvisited_words;
+    uint32_t* queue;                // batched: next-query counter
+};
+
+// ---- exact visited multiset (keys only; duplicates occupy several slots) ----------
+__device__ __forceinline__ uint32_t visited_home(uint32_t id, uint32_t mask) {
+    return (uint32_t)(hash64_2(id) >> 32) & mask;  // reference busqueda.cu:58-60
+}
+
+// warp-cooperative insert: 32 consecutive slots per probe round, first empty wins
+__device__ __forceinline__ void visited_insert(uint32_t* tab, uint32_t mask, uint32_t id,
+                                               int lane) {
+    const uint32_t h = visited_home(id, mask);
+    for (uint32_t probe = 0; probe <= mask; probe += 32) {
+        const uint32_t s = (h + probe + (uint32_t)lane) & mask;
+        const uint32_t empty = __ballot_sync(kFull, tab[s] == kEmptyId);
+        if (empty) {
+            if (lane == __ffs(empty) - 1) tab[s] = id;
+            break;
+        }
+    }
+    __syncwarp();
+}
+
+// number of copies of id (single lane)
+__device__ __forceinline__ int visited_count(const uint32_t* tab, uint32_t mask, uint32_t id) {
+    const uint32_t h = visited_home(id, mask);
+    int c = 0;
+    for (uint32_t i = 0; i <= mask; i++) {
+        const uint32_t v = tab[(h + i) & mask];
+        if (v == kEmptyId) break;
+        c += (v == id);
+    }
+    return c;
+}
+
+// ---- sorted-key searches over shared memory ----------------------------------------
+__device__ __forceinline__ int lower_bound_key(const uint64_t* a, int n, uint64_t key) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ int upper_bound_key(const uint64_t* a, int n, uint64_t key) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (a[mid] <= key) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// ---- warp bitonic sort of 32*E keys held E per lane (element e = t*32 + lane) -------
+template <int E>
+__device__ __forceinline__ void bitonic_sort(uint64_t (&v)[E], int lane) {
+#pragma unroll
+    for (int kk = 2; kk <= 32 * E; kk <<= 1) {
+#pragma unroll
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+#pragma unroll
+                for (int t = 0; t < E; t++) {
+                    const int tp = t ^ (j >> 5);
+                    if (tp > t) {
+                        const bool asc = (((t * 32 + lane) & kk) == 0);
+                        const uint64_t a = v[t], b = v[tp];
+                        const bool sw = asc ? (a > b) : (a < b);
+                        v[t] = sw ? b : a;
+                        v[tp] = sw ? a : b;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int t = 0; t < E; t++) {
+                    const uint64_t o = __shfl_xor_sync(kFull, v[t], j);
+                    const bool asc = (((t * 32 + lane) & kk) == 0);
+                    const bool lower = (lane & j) == 0;
+                    const uint64_t mn = v[t] < o ? v[t] : o;
+                    const uint64_t mx = v[t] < o ? o : v[t];
+                    v[t] = (lower == asc) ? mn : mx;
+                }
+            }
+        }
+    }
+}
+
+template <int E>
+__device__ __forceinline__ void sort_keys_e(uint64_t* keys, int nc, int lane) {
+    uint64_t v[E];
+#pragma unroll
+    for (int t = 0; t < E; t++) {
+        const int e = t * 32 + lane;
+        v[t] = (e < nc) ? keys[e] : kEmptyKey;
+    }
+    bitonic_sort<E>(v, lane);
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < E; t++) {
+        const int e = t * 32 + lane;
+        if (e < nc) keys[e] = v[t];
+    }
+    __syncwarp();
+}
+
+// sorts keys[0..nc) ascending; nc <= 32 * CH
+template <int CH>
+__device__ __forceinline__ void sort_keys(uint64_t* keys, int nc, int lane) {
+    if (nc <= 1) return;
+    if (nc <= 32) {
+        sort_keys_e<1>(keys, nc, lane);
+    } else if (CH >= 2 && nc <= 64) {
+        sort_keys_e<(CH >= 2 ? 2 : 1)>(keys, nc, lane);
+    } else if (CH >= 3 && nc <= 128) {
+        sort_keys_e<(CH >= 3 ? 4 : 1)>(keys, nc, lane);
+    } else {
+        sort_keys_e<(CH >= 5 ? 8 : 1)>(keys, nc, lane);
+    }
+}
+
+// ---- distances of pending rows: 8 lanes per 128-byte row, 16 rows in flight ---------
+template <bool Signed>
+__device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
+                                              const uint32_t* ids, int32_t* out, int np,
+                                              const int4 qv, const int32_t qq, uint32_t dim,
+                                              int lane) {
+    const int grp = lane >> 3, sub = lane & 7;
+    const bool need = (uint32_t)(sub * 16) < dim;  // bytes past dim are zero in every row
+    for (int base = 0; base < np; base += 16) {
+        int4 v[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int i = base + r * 4 + grp;
+            v[r] = make_int4(0, 0, 0, 0);
+            if (i < np && need) v[r] = ldg16(rows + (size_t)ids[i] * kRowBytes + sub * 16);
+        }
+        int32_t t[4];
+#pragma unroll
+        for (int r = 0; r < 4; r++) t[r] = partial_l2<Signed>(v[r], qv);
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+            for (int r = 0; r < 4; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 8);
+        if (sub == 0) {
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int i = base + r * 4 + grp;
+                if (i < np) out[i] = qq + t[r];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// ---- one query -----------------------------------------------------------------------
+// CH: adjacency chunks of 32. SFILT: lossy filter in shared memory (else gfilter).
+// The visited table lives in gvisited when that is non-null, else in shared memory.
+template <int CH, bool Signed, bool SFILT>
+__device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfilter,
+                           uint32_t* gvisited, uint32_t q, uint32_t Ls, uint32_t k, int lane) {
+    const FlatLayout& L = A.L;
+    uint32_t* qwords = reinterpret_cast<uint32_t*>(wmem);
+    uint64_t* fkey = reinterpret_cast<uint64_t*>(wmem + L.off_fkey);
+    uint8_t* fvis = wmem + L.off_fvis;
+    uint32_t* pend = reinterpret_cast<uint32_t*>(wmem + L.off_a);
+    int32_t* pdist = reinterpret_cast<int32_t*>(wmem + L.off_a + 4u * L.gs);
+    uint64_t* ekey = reinterpret_cast<uint64_t*>(wmem + L.off_a);  // reuses pend/pdist
+    uint64_t* ckey = reinterpret_cast<uint64_t*>(wmem + L.off_b);
+    int32_t* epos = reinterpret_cast<int32_t*>(wmem + L.off_c);
+    uint8_t* evis = wmem + L.off_c + 4u * L.gs;
+    uint32_t* filter = SFILT ? reinterpret_cast<uint32_t*>(wmem + L.off_filter) : gfilter;
+    uint32_t* vtab = gvisited ? gvisited : reinterpret_cast<uint32_t*>(wmem + L.off_visited);
+
+    const uint32_t qid = A.qbase + q;
+    const uint32_t fmask = (1u << flat_filter_bits(Ls)) - 1u;
+    const uint32_t vcap = flat_visited_cap(Ls);
+    const uint32_t vmask = vcap - 1u;
+    const int max_visits = (int)(vcap / 2u);
+    const int64_t limit = A.limit;
+    const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
+
+    // query row (zero padded) and ||q||^2
+    load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
+    // clear this query's tables
+    for (uint32_t i = lane; i <= fmask; i += 32) filter[i] = kEmptyId;
+    for (uint32_t i = lane; i < vcap; i += 32) vtab[i] = kEmptyId;
+    __syncwarp();
+    const int4 qv = reinterpret_cast<const int4*>(qwords)[lane & 7];
+    int32_t qq = partial_sq<Signed>(qv);
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) qq += __shfl_xor_sync(kFull, qq, off, 8);
+
+    // start point: F = {(d(q, start), start)}, one distance
+    if (lane == 0) pend[0] = A.start;
+    __syncwarp();
+    row_distances<Signed>(A.rows, pend, pdist, 1, qv, qq, A.dim, lane);
+    if (lane == 0) {
+        fkey[0] = pack_key(pdist[0], A.start);
+        fvis[0] = 0;
+    }
+    __syncwarp();
+
+    int fsize = 1, u = 0, flags = 0;
+    int nvis = 0;
+    int comps = 1;
+    const int deg_lim = (int)A.deg_lim;
+
+    while (u >= 0 && (int64_t)nvis < limit) {
+        const uint64_t cur_key = fkey[u];
+        const uint32_t cur = key_id(cur_key);
+        // whole neighbour row, requested before it is needed
+        uint32_t a[CH];
+        const uint32_t* row = A.adj + (size_t)cur * A.gs;
+#pragma unroll
+        for (int t = 0; t < CH; t++) {
+            const int j = t * 32 + lane;
+            a[t] = (j < deg_lim) ? __ldg(row + j) : kEmptyId;
+        }
+        if (lane == 0) fvis[u] = 1;
+        visited_insert(vtab, vmask, cur, lane);
+        nvis++;
+        if (nvis > max_visits) {
+            flags |= PGB_FLAG_OVERFLOW;
+            break;
+        }
+        const int32_t cutoff = (fsize < (int)Ls) ? INT_MAX : key_dist(fkey[fsize - 1]);
+
+        // ---- lossy filter in row order -> pending ids ------------------------------
+        int np = 0;
+        if (SFILT) {
+            // chunks in order: each chunk sees the writes of the previous ones
+#pragma unroll
+            for (int t = 0; t < CH; t++) {
+                const uint32_t x = a[t];
+                const bool part = x != kEmptyId && !(A.excl && x == qid);
+                const uint32_t slot =
+                    part ? (uint32_t)(hash64_2(x) & fmask) : (0x80000000u | (uint32_t)(t * 32 + lane));
+                const uint32_t peers = __match_any_sync(kFull, slot);
+                const uint32_t before = peers & lt;
+                const int src = before ? 31 - __clz(before) : lane;
+                const uint32_t prev = __shfl_sync(kFull, x, src);
+                bool seen;
+                if (before) seen = part && prev == x;
+                else seen = part && filter[slot] == x;
+                __syncwarp();
+                if (part && (peers & gt) == 0) filter[slot] = x;
+                const bool pass = part && !seen;
+                const uint32_t m = __ballot_sync(kFull, pass);
+                if (pass) pend[np + __popc(m & lt)] = x;
+                np += __popc(m);
+                __syncwarp();
+            }
+        } else {
+            // global table: all slots read up front (one round trip); an entry with no
+            // earlier same-slot entry in its chunk takes the value written by the last
+            // earlier chunk entry of that slot, else the table value
+            uint32_t slot[CH], mem[CH];
+#pragma unroll
+            for (int t = 0; t < CH; t++) {
+                const uint32_t x = a[t];
+                const bool part = x != kEmptyId && !(A.excl && x == qid);
+                slot[t] = part ? (uint32_t)(hash64_2(x) & fmask)
+                               : (0x80000000u | (uint32_t)(t * 32 + lane));
+                mem[t] = part ? filter[slot[t]] : kEmptyId;
+            }
+            uint32_t* sslot = reinterpret_cast<uint32_t*>(ckey);  // scratch: slots of row
+            uint32_t* sid = sslot + 32 * CH;                        // and ids
+#pragma unroll
+            for (int t = 0; t < CH; t++) {
+                const uint32_t x = a[t];
+                const bool part = x != kEmptyId && !(A.excl && x == qid);
+                const uint32_t peers = __match_any_sync(kFull, slot[t]);
+                const uint32_t before = peers & lt;
+                const int src = before ? 31 - __clz(before) : lane;
+                const uint32_t prev = __shfl_sync(kFull, x, src);
+                bool seen;
+                if (before) {
+                    seen = part && prev == x;
+                } else {
+                    seen = part && mem[t] == x;
+                    if (part)
+                        for (int p = t * 32 - 1; p >= 0; p--)
+                            if (sslot[p] == slot[t]) {
+                                seen = sid[p] == x;
+                                break;
+                            }
+                }
+                __syncwarp();
+                sslot[t * 32 + lane] = slot[t];
+                sid[t * 32 + lane] = x;
+                if (part && (peers & gt) == 0) filter[slot[t]] = x;
+                const bool pass = part && !seen;
+                const uint32_t m = __ballot_sync(kFull, pass);
+                if (pass) pend[np + __popc(m & lt)] = x;
+                np += __popc(m);
+                __syncwarp();
+            }
+        }
+        comps += np;
+
+        // ---- distances ------------------------------------------------------------
+        row_distances<Signed>(A.rows, pend, pdist, np, qv, qq, A.dim, lane);
+
+        // ---- candidates under the cutoff, in arrival order ------------------------
+        int nc = 0;
+        for (int base = 0; base < np; base += 32) {
+            const int i = base + lane;
+            const bool c = i < np && pdist[i] < cutoff;
+            const uint32_t m = __ballot_sync(kFull, c);
+            if (c) ckey[nc + __popc(m & lt)] = pack_key(pdist[i], pend[i]);
+            nc += __popc(m);
+        }
+        __syncwarp();
+
+        int unew = u, minpos = INT_MAX;
+        if (nc > 0) {
+            sort_keys<CH>(ckey, nc, lane);
+            // ---- multiset set_union: copy `rep` of a key enters iff rep >= copies in F
+            int ne = 0;
+            for (int base = 0; base < nc; base += 32) {
+                const int i = base + lane;
+                bool enter = false;
+                int hi = 0;
+                uint64_t key = 0;
+                uint8_t vis = 0;
+                if (i < nc) {
+                    key = ckey[i];
+                    hi = upper_bound_key(fkey, fsize, key);
+                    int cf = 0;
+                    if (hi > 0 && fkey[hi - 1] == key) cf = hi - lower_bound_key(fkey, fsize, key);
+                    int rep = 0;
+                    while (i - rep - 1 >= 0 && ckey[i - rep - 1] == key) rep++;
+                    enter = rep >= cf;
+                    if (enter)
+                        vis = (uint8_t)(rep < visited_count(vtab, vmask, key_id(key)));
+                }
+                const uint32_t m = __ballot_sync(kFull, enter);
+                // new copies follow the frontier copies of an equal key
+                const int pos = hi + ne + __popc(m & lt);
+                const bool keep = enter && pos < (int)Ls;
+                const uint32_t mk = __ballot_sync(kFull, keep);
+                if (keep) {
+                    const int jk = ne + __popc(mk & lt);
+                    ekey[jk] = key;
+                    epos[jk] = pos;
+                    evis[jk] = vis;
+                }
+                ne += __popc(mk);
+                if (mk != m) break;  // later keys land at or past Ls
+            }
+            __syncwarp();
+            if (ne > 0) {
+                // the expanded entry's new position, then shift the frontier tail
+                unew = u + lower_bound_key(ekey, ne, cur_key);
+                const int first = epos[0];
+                for (int top = fsize - 1; top >= first; top -= 32) {
+                    const int i = top - lane;
+                    const bool act = i >= first;
+                    uint64_t key = 0;
+                    uint8_t vis = 0;
+                    int np2 = 0;
+                    if (act) {
+                        key = fkey[i];
+                        vis = fvis[i];
+                        np2 = i + lower_bound_key(ekey, ne, key);
+                    }
+                    __syncwarp();
+                    if (act && np2 < (int)Ls) {
+                        fkey[np2] = key;
+                        fvis[np2] = vis;
+                    }
+                    __syncwarp();
+                }
+                for (int j = lane; j < ne; j += 32) {
+                    fkey[epos[j]] = ekey[j];
+                    fvis[epos[j]] = evis[j];
+                    if (!evis[j]) minpos = min(minpos, epos[j]);
+                }
+                __syncwarp();
+                fsize = min((int)Ls, fsize + ne);
+            }
+        }
+
+        // ---- cut --------------------------------------------------------------------
+        if (fsize > (int)k) {
+            const float thr = (float)(A.cut * (double)key_dist(fkey[k]));
+            int newsize = fsize;
+            for (int base = 0; base < fsize; base += 32) {
+                const int i = base + lane;
+                bool after = false;
+                if (i < fsize) {
+                    const uint64_t e = fkey[i];
+                    const float de = (float)key_dist(e);
+                    after = thr < de || (thr == de && 0u < key_id(e));
+                }
+                const uint32_t m = __ballot_sync(kFull, after);
+                if (m) {
+                    newsize = base + __ffs(m) - 1;
+                    break;
+                }
+            }
+            fsize = newsize;
+        }
+
+        // ---- next unvisited ---------------------------------------------------------
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) minpos = min(minpos, __shfl_xor_sync(kFull, minpos, off));
+        const int from = min(unew, minpos);
+        u = -1;
+        for (int base = from; base < fsize; base += 32) {
+            const int i = base + lane;
+            const bool un = i < fsize && !fvis[i];
+            const uint32_t m = __ballot_sync(kFull, un);
+            if (m) {
+                u = base + __ffs(m) - 1;
+                break;
+            }
+        }
+        __syncwarp();
+    }
+
+    // ---- output: first k of the frontier ----------------------------------------------
+    if (fsize < (int)k) flags |= PGB_FLAG_SHORT;
+    uint32_t* oid = A.ids + (size_t)q * A.out_stride;
+    int32_t* od = A.dists + (size_t)q * A.out_stride;
+    for (uint32_t j = lane; j < k; j += 32) {
+        const bool have = (int)j < fsize;
+        const uint64_t e = have ? fkey[j] : 0;
+        oid[j] = have ? key_id(e) : kEmptyId;
+        od[j] = have ? key_dist(e) : INT_MAX;
+    }
+    if (lane == 0 && A.stats) {
+        pgb_query_stats s;
+        s.dist_comps = comps;
+        s.expansions = nvis;
+        s.flags = flags;
+        s.reserved = 0;
+        A.stats[q] = s;
+    }
+    __syncwarp();
+}
+
+}  // namespace pgb

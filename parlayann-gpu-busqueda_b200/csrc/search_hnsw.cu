@@ -1,0 +1,615 @@
+// search_hnsw.cu -- HNSW layered search, one warp per query.
+//
+// Semantics follow the reference's HNSW kernel (cuda/busqueda_hnsw.cu:215-456), itself
+// ParlayANN's HNSW::search: per layer from the top, ef = 1 and 2 filter bits above
+// layer 0, ef = Ls and bits0 = 2*ceil(log2 Ls) - 2 on layer 0 with limit_eval; entry
+// points marked with hash64, neighbours with hash64_2; cand ordered by distance only
+// (equal distances rejected); workset W ordered by (dist, id); is_inw exact; next
+// layer's entry = W's worst; output the first k of W mapped node -> point.
+//
+// The reference decides acceptance neighbour by neighbour (:400-418). Here the
+// decisions are made lane-parallel from a closed form that yields the same set:
+// with m = max(ef, |W|), neighbour j is accepted iff it is eligible (not in is_inw and
+// the first copy of its id among this expansion's survivors) and fewer than m elements
+// of W plus the eligible neighbours before j have distance <= d_j. (A rejected
+// neighbour has d >= the current worst, so counting it never moves the threshold.)
+// W then becomes the smallest m' = min(m, |W| + accepted) of W + accepted, and cand the
+// ef smallest distinct distances of cand + accepted (first copy of each distance
+// wins); when cand starts above ef (several entry points on the top layer) its
+// per-neighbour trim rule is replayed sequentially instead.
+#include <algorithm>
+#include <climits>
+#include <string>
+
+#include "errors.h"
+#include "index.h"
+#include "search_flat.cuh"
+#include "search_hnsw.h"
+#include "search_plan.h"
+
+namespace pgb {
+
+__host__ __device__ inline uint32_t hnsw_bits0(uint32_t Ls) {
+    return Ls > 2 ? 2u * (uint32_t)ceil_log2_u64(Ls) - 2u : 2u;  // busqueda_hnsw.cu:556-557
+}
+__host__ __device__ inline uint32_t hnsw_cap_inw(uint32_t Ls) {
+    return next_pow2_u32(32u * Ls + 2048u);  // busqueda_hnsw.cu:559
+}
+
+struct HnswLayout {
+    uint32_t wcap, gs, filter_words;
+    uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_filter,
+        bytes;
+};
+
+__host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t gs,
+                                                       uint32_t filter_words) {
+    HnswLayout L;
+    L.wcap = wcap;
+    L.gs = gs;
+    L.filter_words = filter_words;
+    uint32_t o = kRowBytes;
+    L.off_w = o;
+    o += 8u * wcap;
+    L.off_c = o;
+    o += 8u * wcap;
+    L.off_pend = o;
+    o += 4u * gs;
+    L.off_pd = o;
+    o += 4u * gs;
+    L.off_ak = o;
+    o += 8u * gs;
+    L.off_nk = o;
+    o += 8u * gs;
+    L.off_pos = o;
+    o += 4u * gs;
+    L.off_fl = o;
+    o = round16(o + gs);
+    L.off_eps = o;
+    o += 4u * PGB_MAX_HNSW_ENTRIES;
+    L.off_filter = o;
+    o += 4u * filter_words;
+    L.bytes = round16(o);
+    return L;
+}
+
+struct HnswArgs {
+    const uint8_t* rows;  // node order
+    const uint32_t* adj0;
+    uint32_t g0s, G0;
+    const uint32_t* adju;
+    uint32_t gas, GA;
+    const uint32_t* upper_start;
+    const uint32_t* node_point;
+    uint32_t entries[PGB_MAX_HNSW_ENTRIES];
+    uint32_t n_entries, top, dim;
+    const uint8_t* queries;
+    uint32_t nq, qstride;
+    uint32_t Ls, k;
+    uint64_t limit0;
+    uint32_t bits0, cap_inw, filter_slots;
+    HnswLayout L;
+    uint32_t* ids;
+    int32_t* dists;
+    pgb_query_stats* stats;
+    unsigned long long* inw;
+    unsigned long long* gfilter;
+    uint64_t epoch_base;
+};
+
+__device__ __forceinline__ unsigned long long tag(uint32_t epoch, uint32_t id) {
+    return ((unsigned long long)epoch << 32) | id;
+}
+
+// is_inw: exact set, epoch-tagged slots (a slot of an older epoch is empty)
+__device__ bool inw_contains(const unsigned long long* tab, uint32_t mask, uint32_t epoch,
+                             uint32_t id) {
+    uint32_t h = (uint32_t)(hash64_2(id) >> 32) & mask;
+    const unsigned long long want = tag(epoch, id);
+    for (uint32_t i = 0; i <= mask; i++) {
+        const unsigned long long c = __ldcg(tab + h);
+        if (c == want) return true;
+        if ((uint32_t)(c >> 32) != epoch) return false;
+        h = (h + 1) & mask;
+    }
+    return false;
+}
+
+// concurrent inserts of distinct ids by several lanes
+__device__ void inw_insert(unsigned long long* tab, uint32_t mask, uint32_t epoch, uint32_t id) {
+    uint32_t h = (uint32_t)(hash64_2(id) >> 32) & mask;
+    const unsigned long long want = tag(epoch, id);
+    for (uint32_t i = 0; i <= 2 * mask + 1; i++) {
+        const unsigned long long c = __ldcg(tab + h);
+        if (c == want) return;
+        if ((uint32_t)(c >> 32) != epoch) {
+            const unsigned long long old = atomicCAS(tab + h, c, want);
+            if (old == c || old == want) return;
+            continue;  // slot taken meanwhile: look at it again
+        }
+        h = (h + 1) & mask;
+    }
+}
+
+template <int CH, bool Signed, bool SFILT>
+__global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t gw = blockIdx.x * wpb + w;
+    const uint32_t total = gridDim.x * wpb;
+    const HnswLayout& L = A.L;
+    unsigned char* wmem = smem + (size_t)w * L.bytes;
+    uint32_t* qwords = reinterpret_cast<uint32_t*>(wmem);
+    uint64_t* wkey = reinterpret_cast<uint64_t*>(wmem + L.off_w);
+    uint64_t* ckey = reinterpret_cast<uint64_t*>(wmem + L.off_c);
+    uint32_t* pend = reinterpret_cast<uint32_t*>(wmem + L.off_pend);
+    int32_t* pd = reinterpret_cast<int32_t*>(wmem + L.off_pd);
+    uint64_t* akey = reinterpret_cast<uint64_t*>(wmem + L.off_ak);
+    uint64_t* nkey = reinterpret_cast<uint64_t*>(wmem + L.off_nk);
+    int32_t* pos = reinterpret_cast<int32_t*>(wmem + L.off_pos);
+    uint8_t* fl = wmem + L.off_fl;
+    uint32_t* eps = reinterpret_cast<uint32_t*>(wmem + L.off_eps);
+    uint32_t* sfilter = reinterpret_cast<uint32_t*>(wmem + L.off_filter);
+    unsigned long long* inw = A.inw + (size_t)gw * A.cap_inw;
+    unsigned long long* gfil = SFILT ? nullptr : A.gfilter + (size_t)gw * A.filter_slots;
+    const uint32_t inw_mask = A.cap_inw - 1u;
+    const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
+    const uint32_t layers = A.top + 1u;
+
+    for (uint32_t q = gw; q < A.nq; q += total) {
+        load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
+        __syncwarp();
+        const int4 qv = reinterpret_cast<const int4*>(qwords)[lane & 7];
+        int32_t qq = partial_sq<Signed>(qv);
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) qq += __shfl_xor_sync(kFull, qq, off, 8);
+
+        int comps = 0, exps = 0, flags = 0;
+        int neps = (int)A.n_entries;
+        if (lane < neps) eps[lane] = A.entries[lane];
+        __syncwarp();
+        int nW = 0;
+
+        for (int layer = (int)A.top; layer >= 0; layer--) {
+            const int ef = (layer > 0) ? 1 : (int)A.Ls;
+            const uint32_t bits = (layer > 0) ? 2u : A.bits0;
+            const uint32_t fmask = (1u << bits) - 1u;
+            const uint64_t limit = (layer > 0) ? ~0ull : A.limit0;
+            const uint32_t* mat = (layer > 0) ? A.adju : A.adj0;
+            const uint32_t stride = (layer > 0) ? A.gas : A.g0s;
+            const int G = (int)((layer > 0) ? A.GA : A.G0);
+            const uint32_t epoch =
+                (uint32_t)(A.epoch_base + (uint64_t)q * layers + (A.top - (uint32_t)layer) + 1u);
+            if (SFILT) {
+                for (uint32_t i = lane; i <= fmask; i += 32) sfilter[i] = kEmptyId;
+                __syncwarp();
+            }
+            // ---- entry points: distances, then the sequential inserts on lane 0 ----
+            for (int e = lane; e < neps; e += 32) pend[e] = eps[e];
+            __syncwarp();
+            row_distances<Signed>(A.rows, pend, pd, neps, qv, qq, A.dim, lane);
+            int nC = 0;
+            nW = 0;
+            if (lane == 0) {
+                for (int e = 0; e < neps; e++) {
+                    const uint32_t pe = pend[e];
+                    const int32_t d = pd[e];
+                    const uint32_t s = (uint32_t)(hash64(pe) & fmask);
+                    if (SFILT) sfilter[s] = pe;
+                    else gfil[s] = tag(epoch, pe);
+                    inw_insert(inw, inw_mask, epoch, pe);
+                    // cand: by distance, equal distance rejected
+                    const uint64_t key = pack_key(d, pe);
+                    int pos = lower_bound_key(ckey, nC, pack_key(d, 0));
+                    if (!(pos < nC && key_dist(ckey[pos]) == d)) {
+                        for (int i = nC; i > pos; i--) ckey[i] = ckey[i - 1];
+                        ckey[pos] = key;
+                        nC++;
+                    }
+                    // W: (dist, id) order, no trim
+                    pos = upper_bound_key(wkey, nW, key);
+                    for (int i = nW; i > pos; i--) wkey[i] = wkey[i - 1];
+                    wkey[pos] = key;
+                    nW++;
+                }
+            }
+            nC = __shfl_sync(kFull, nC, 0);
+            nW = __shfl_sync(kFull, nW, 0);
+            __syncwarp();
+            comps += neps;
+            uint32_t inserted = (uint32_t)neps;
+            uint64_t cnt = 0;
+
+            while (nC > 0) {
+                if (key_dist(ckey[0]) > key_dist(wkey[nW - 1])) break;
+                if (++cnt > limit) break;
+                const uint32_t u = key_id(ckey[0]);
+                // pop the closest candidate
+                for (int base = 0; base < nC - 1; base += 32) {
+                    const int i = base + lane;
+                    uint64_t v = 0;
+                    if (i + 1 < nC) v = ckey[i + 1];
+                    __syncwarp();
+                    if (i + 1 < nC) ckey[i] = v;
+                    __syncwarp();
+                }
+                nC--;
+                exps++;
+                const uint32_t* row =
+                    (layer > 0) ? mat + ((size_t)A.upper_start[u] + (uint32_t)(layer - 1)) * stride
+                                : mat + (size_t)u * stride;
+                uint32_t a[CH];
+#pragma unroll
+                for (int t = 0; t < CH; t++) {
+                    const int j = t * 32 + lane;
+                    a[t] = (j < G) ? __ldg(row + j) : kEmptyId;
+                }
+                // ---- lossy visited filter in row order ---------------------------------
+                int np = 0;
+                if (SFILT) {
+#pragma unroll
+                    for (int t = 0; t < CH; t++) {
+                        const uint32_t x = a[t];
+                        const bool part = x != kEmptyId;
+                        const uint32_t slot = part ? (uint32_t)(hash64_2(x) & fmask)
+                                                   : (0x80000000u | (uint32_t)(t * 32 + lane));
+                        const uint32_t peers = __match_any_sync(kFull, slot);
+                        const uint32_t before = peers & lt;
+                        const int src = before ? 31 - __clz(before) : lane;
+                        const uint32_t prev = __shfl_sync(kFull, x, src);
+                        bool seen;
+                        if (before) seen = part && prev == x;
+                        else seen = part && sfilter[slot] == x;
+                        __syncwarp();
+                        if (part && (peers & gt) == 0) sfilter[slot] = x;
+                        const bool pass = part && !seen;
+                        const uint32_t m = __ballot_sync(kFull, pass);
+                        if (pass) pend[np + __popc(m & lt)] = x;
+                        np += __popc(m);
+                        __syncwarp();
+                    }
+                } else {
+                    uint32_t slot[CH];
+                    unsigned long long mem[CH];
+#pragma unroll
+                    for (int t = 0; t < CH; t++) {
+                        const bool part = a[t] != kEmptyId;
+                        slot[t] = part ? (uint32_t)(hash64_2(a[t]) & fmask)
+                                       : (0x80000000u | (uint32_t)(t * 32 + lane));
+                        mem[t] = part ? __ldcg(gfil + slot[t]) : 0ull;
+                    }
+                    uint32_t* sslot = reinterpret_cast<uint32_t*>(akey);
+                    uint32_t* sid = sslot + 32 * CH;
+#pragma unroll
+                    for (int t = 0; t < CH; t++) {
+                        const uint32_t x = a[t];
+                        const bool part = x != kEmptyId;
+                        const uint32_t peers = __match_any_sync(kFull, slot[t]);
+                        const uint32_t before = peers & lt;
+                        const int src = before ? 31 - __clz(before) : lane;
+                        const uint32_t prev = __shfl_sync(kFull, x, src);
+                        bool seen;
+                        if (before) {
+                            seen = part && prev == x;
+                        } else {
+                            seen = part && mem[t] == tag(epoch, x);
+                            if (part)
+                                for (int p = t * 32 - 1; p >= 0; p--)
+                                    if (sslot[p] == slot[t]) {
+                                        seen = sid[p] == x;
+                                        break;
+                                    }
+                        }
+                        __syncwarp();
+                        sslot[t * 32 + lane] = slot[t];
+                        sid[t * 32 + lane] = x;
+                        if (part && (peers & gt) == 0) gfil[slot[t]] = tag(epoch, x);
+                        const bool pass = part && !seen;
+                        const uint32_t m = __ballot_sync(kFull, pass);
+                        if (pass) pend[np + __popc(m & lt)] = x;
+                        np += __popc(m);
+                        __syncwarp();
+                    }
+                }
+                comps += np;
+                row_distances<Signed>(A.rows, pend, pd, np, qv, qq, A.dim, lane);
+
+                // ---- eligibility: first copy in this expansion and not in is_inw ------
+                for (int j = lane; j < np; j += 32) {
+                    const uint32_t pv = pend[j];
+                    bool first = true;
+                    for (int i = 0; i < j; i++)
+                        if (pend[i] == pv) {
+                            first = false;
+                            break;
+                        }
+                    fl[j] = (first && !inw_contains(inw, inw_mask, epoch, pv)) ? 1 : 0;
+                }
+                __syncwarp();
+                // ---- acceptance: fewer than m elements of W + earlier eligible at <= d
+                const int m = max(ef, nW);
+                int na = 0;
+                for (int base = 0; base < np; base += 32) {
+                    const int j = base + lane;
+                    bool acc = false;
+                    int32_t d = 0;
+                    uint32_t pv = 0;
+                    if (j < np && fl[j]) {
+                        d = pd[j];
+                        pv = pend[j];
+                        int c = lower_bound_key(wkey, nW, pack_key(d + 1, 0));
+                        for (int i = 0; i < j && c < m; i++) c += (fl[i] && pd[i] <= d) ? 1 : 0;
+                        acc = c < m;
+                    }
+                    const uint32_t mk = __ballot_sync(kFull, acc);
+                    if (acc) akey[na + __popc(mk & lt)] = pack_key(d, pv);
+                    na += __popc(mk);
+                }
+                __syncwarp();
+                if (na > 0) {
+                    inserted += (uint32_t)na;
+                    for (int j = lane; j < na; j += 32) inw_insert(inw, inw_mask, epoch, key_id(akey[j]));
+                    // ---- cand update (accepted keys still in arrival order) ---------------
+                    const int nC0 = nC;
+                    if (nC0 <= ef) {
+                        // new distances only, first copy of each distance
+                        int nn = 0;
+                        for (int base = 0; base < na; base += 32) {
+                            const int j = base + lane;
+                            bool nw = false;
+                            uint64_t key = 0;
+                            if (j < na) {
+                                key = akey[j];
+                                const int32_t d = key_dist(key);
+                                const int p = lower_bound_key(ckey, nC0, pack_key(d, 0));
+                                nw = !(p < nC0 && key_dist(ckey[p]) == d);
+                                for (int i = 0; i < j && nw; i++)
+                                    if (key_dist(akey[i]) == d) nw = false;
+                            }
+                            const uint32_t mk = __ballot_sync(kFull, nw);
+                            if (nw) nkey[nn + __popc(mk & lt)] = key;
+                            nn += __popc(mk);
+                        }
+                        __syncwarp();
+                        if (nn > 0) {
+                            sort_keys<CH>(nkey, nn, lane);
+                            const int nCn = min(ef, nC0 + nn);
+                            for (int j = lane; j < nn; j += 32)
+                                pos[j] = lower_bound_key(ckey, nC0, pack_key(key_dist(nkey[j]), 0)) + j;
+                            __syncwarp();
+                            const int first = pos[0];
+                            for (int topi = nC0 - 1; topi >= first; topi -= 32) {
+                                const int i = topi - lane;
+                                const bool act = i >= first;
+                                uint64_t key = 0;
+                                int np2 = 0;
+                                if (act) {
+                                    key = ckey[i];
+                                    np2 = i + lower_bound_key(nkey, nn, pack_key(key_dist(key), 0));
+                                }
+                                __syncwarp();
+                                if (act && np2 < nCn) ckey[np2] = key;
+                                __syncwarp();
+                            }
+                            for (int j = lane; j < nn; j += 32)
+                                if (pos[j] < nCn) ckey[pos[j]] = nkey[j];
+                            __syncwarp();
+                            nC = nCn;
+                        }
+                    } else if (lane == 0) {
+                        // cand above ef (several top-layer entries): replay the rule
+                        for (int j = 0; j < na; j++) {
+                            const uint64_t key = akey[j];
+                            const int32_t d = key_dist(key);
+                            const int p = lower_bound_key(ckey, nC, pack_key(d, 0));
+                            if (!(p < nC && key_dist(ckey[p]) == d)) {
+                                for (int i = nC; i > p; i--) ckey[i] = ckey[i - 1];
+                                ckey[p] = key;
+                                nC++;
+                            }
+                            if (nC > ef) nC--;
+                        }
+                    }
+                    nC = __shfl_sync(kFull, nC, 0);
+                    __syncwarp();
+                    // ---- W update: the m' smallest of W + accepted -----------------------
+                    sort_keys<CH>(akey, na, lane);
+                    const int nWn = min(m, nW + na);
+                    for (int j = lane; j < na; j += 32) pos[j] = upper_bound_key(wkey, nW, akey[j]) + j;
+                    __syncwarp();
+                    const int firstw = pos[0];
+                    for (int topi = nW - 1; topi >= firstw; topi -= 32) {
+                        const int i = topi - lane;
+                        const bool act = i >= firstw;
+                        uint64_t key = 0;
+                        int np2 = 0;
+                        if (act) {
+                            key = wkey[i];
+                            np2 = i + lower_bound_key(akey, na, key);
+                        }
+                        __syncwarp();
+                        if (act && np2 < nWn) wkey[np2] = key;
+                        __syncwarp();
+                    }
+                    for (int j = lane; j < na; j += 32)
+                        if (pos[j] < nWn) wkey[pos[j]] = akey[j];
+                    __syncwarp();
+                    nW = nWn;
+                }
+                if (inserted > A.cap_inw / 2) {
+                    flags |= PGB_FLAG_OVERFLOW;
+                    break;
+                }
+            }
+            if (layer > 0) {
+                if (lane == 0) eps[0] = key_id(wkey[nW - 1]);
+                neps = 1;
+                __syncwarp();
+            }
+        }
+        // ---- output: first k of W, node -> point ------------------------------------
+        if (nW < (int)A.k) flags |= PGB_FLAG_SHORT;
+        uint32_t* oid = A.ids + (size_t)q * A.k;
+        int32_t* od = A.dists + (size_t)q * A.k;
+        for (uint32_t j = lane; j < A.k; j += 32) {
+            const bool have = (int)j < nW;
+            const uint64_t e = have ? wkey[j] : 0;
+            oid[j] = have ? A.node_point[key_id(e)] : kEmptyId;
+            od[j] = have ? key_dist(e) : INT_MAX;
+        }
+        if (lane == 0 && A.stats) {
+            pgb_query_stats s;
+            s.dist_comps = comps;
+            s.expansions = exps;
+            s.flags = flags;
+            s.reserved = 0;
+            A.stats[q] = s;
+        }
+        __syncwarp();
+    }
+}
+
+}  // namespace pgb
+
+namespace pgb {
+namespace {
+
+using HnswKernel = void (*)(HnswArgs);
+
+template <int CH>
+HnswKernel pick_hnsw_ch(bool is_signed, bool sfilt) {
+    if (is_signed) return sfilt ? hnsw_kernel<CH, true, true> : hnsw_kernel<CH, true, false>;
+    return sfilt ? hnsw_kernel<CH, false, true> : hnsw_kernel<CH, false, false>;
+}
+
+HnswKernel pick_hnsw(int ch, bool is_signed, bool sfilt) {
+    switch (ch) {
+        case 1: return pick_hnsw_ch<1>(is_signed, sfilt);
+        case 2: return pick_hnsw_ch<2>(is_signed, sfilt);
+        case 3: return pick_hnsw_ch<3>(is_signed, sfilt);
+        case 4: return pick_hnsw_ch<4>(is_signed, sfilt);
+        default: return pick_hnsw_ch<8>(is_signed, sfilt);
+    }
+}
+
+pgb_status hnsw_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return PGB_OK;
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation) return fail(PGB_ERR_OOM, std::string(what) + ": out of memory");
+    return fail(PGB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswState& H) {
+    H = HnswState{};
+    const uint32_t Ls = p.beam_size;
+    H.ch = flat_chunks_for(std::max(ix->G0, ix->GA));
+    H.bits0 = hnsw_bits0(Ls);
+    H.cap_inw = hnsw_cap_inw(Ls);
+    const uint32_t fwords = 1u << H.bits0;
+    H.sfilt = 4ull * fwords <= 16384;
+    H.filter_slots = H.sfilt ? 0u : fwords;
+    H.wcap = ((std::max<uint32_t>(Ls, PGB_MAX_HNSW_ENTRIES) + 8u) + 7u) & ~7u;
+    const HnswLayout L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? fwords : 0u);
+    H.warp_bytes = L.bytes;
+    H.kernel = (void*)pick_hnsw(H.ch, ix->elem == PGB_INT8, H.sfilt);
+    cudaDeviceProp prop;
+    int dev = 0;
+    pgb_status s;
+    if ((s = hnsw_cuda(cudaGetDevice(&dev), "cudaGetDevice")) != PGB_OK) return s;
+    if ((s = hnsw_cuda(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties")) != PGB_OK) return s;
+    int wpb = 4;
+    while (wpb > 1 && (size_t)wpb * L.bytes > prop.sharedMemPerBlockOptin) wpb >>= 1;
+    if ((size_t)wpb * L.bytes > prop.sharedMemPerBlockOptin)
+        return fail(PGB_ERR_BAD_ARG, "beam too wide for shared memory");
+    H.warps_per_block = wpb;
+    H.smem_bytes = (size_t)wpb * L.bytes;
+    if ((s = hnsw_cuda(cudaFuncSetAttribute(H.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)H.smem_bytes),
+                       "cudaFuncSetAttribute")) != PGB_OK)
+        return s;
+    int bps = 0;
+    if ((s = hnsw_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, H.kernel, wpb * 32, H.smem_bytes),
+                       "occupancy")) != PGB_OK)
+        return s;
+    if (bps < 1) return fail(PGB_ERR_CUDA, "HNSW kernel does not fit on a multiprocessor");
+    H.blocks = bps * prop.multiProcessorCount;
+    H.total_warps = (uint64_t)H.blocks * wpb;
+    const size_t inw_bytes = 8ull * H.cap_inw * H.total_warps;
+    if ((s = hnsw_cuda(cudaMalloc(&H.inw, inw_bytes), "is_inw tables")) != PGB_OK) return s;
+    if ((s = hnsw_cuda(cudaMemset(H.inw, 0, inw_bytes), "is_inw clear")) != PGB_OK) return s;
+    if (!H.sfilt) {
+        const size_t fb = 8ull * H.filter_slots * H.total_warps;
+        if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, fb), "filter tables")) != PGB_OK) return s;
+        if ((s = hnsw_cuda(cudaMemset(H.gfilter, 0, fb), "filter clear")) != PGB_OK) return s;
+    }
+    H.epoch_base = 0;
+    H.ready = true;
+    return PGB_OK;
+}
+
+pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params& p,
+                       const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
+                       int32_t* dists, pgb_query_stats* stats, cudaStream_t stream) {
+    if (!H.ready) return fail(PGB_ERR_BAD_ARG, "HNSW searcher not prepared");
+    HnswArgs A{};
+    A.rows = ix->node_rows;
+    A.adj0 = ix->adj0;
+    A.g0s = ix->g0s;
+    A.G0 = ix->G0;
+    A.adju = ix->adju;
+    A.gas = ix->gas;
+    A.GA = ix->GA;
+    A.upper_start = ix->upper_start;
+    A.node_point = ix->node_point;
+    for (uint32_t e = 0; e < ix->n_entries; e++) A.entries[e] = ix->entries[e];
+    A.n_entries = ix->n_entries;
+    A.top = ix->top_level;
+    A.dim = ix->dim;
+    A.queries = (const uint8_t*)queries;
+    A.nq = nq;
+    A.qstride = qstride;
+    A.Ls = p.beam_size;
+    A.k = p.k;
+    // limit_eval on layer 0: the visit limit when set below n, else n (busqueda_hnsw.cu:610)
+    A.limit0 = (p.limit > 0 && (uint64_t)p.limit < ix->n_nodes) ? (uint64_t)p.limit : ix->n_nodes;
+    A.bits0 = H.bits0;
+    A.cap_inw = H.cap_inw;
+    A.filter_slots = H.filter_slots;
+    A.L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? (1u << H.bits0) : 0u);
+    A.ids = ids;
+    A.dists = dists;
+    A.stats = stats;
+    A.inw = H.inw;
+    A.gfilter = H.gfilter;
+    // every (query, layer) of every launch gets a fresh epoch; wrap -> clear the tables
+    const uint64_t need = (uint64_t)nq * (ix->top_level + 1ull) + 1ull;
+    if (H.epoch_base + need >= 0xFFFFFFFFull) {
+        pgb_status s;
+        if ((s = hnsw_cuda(cudaMemsetAsync(H.inw, 0, 8ull * H.cap_inw * H.total_warps, stream),
+                           "is_inw clear")) != PGB_OK)
+            return s;
+        if (H.gfilter &&
+            (s = hnsw_cuda(cudaMemsetAsync(H.gfilter, 0, 8ull * H.filter_slots * H.total_warps, stream),
+                           "filter clear")) != PGB_OK)
+            return s;
+        H.epoch_base = 0;
+    }
+    A.epoch_base = H.epoch_base;
+    H.epoch_base += need;
+    void* args[] = {&A};
+    cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
+                                     H.smem_bytes, stream);
+    return hnsw_cuda(e, "HNSW launch");
+}
+
+void hnsw_release(HnswState& H) {
+    cudaFree(H.inw);
+    cudaFree(H.gfilter);
+    H = HnswState{};
+}
+
+}  // namespace pgb

@@ -1,0 +1,38 @@
+// search_hnsw.h -- HNSW searcher state (scratch, epochs) and launch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/pgb.h"
+
+struct pgb_index;
+
+namespace pgb {
+
+struct HnswState {
+    bool ready = false;
+    int ch = 1;
+    bool sfilt = true;
+    uint32_t bits0 = 2;         // layer-0 filter bits
+    uint32_t cap_inw = 0;       // is_inw slots (power of two)
+    uint32_t filter_slots = 0;  // global filter slots per warp (0: shared)
+    uint32_t wcap = 0;          // workset / candidate capacity
+    uint32_t warp_bytes = 0;
+    int warps_per_block = 4, blocks = 1;
+    uint64_t total_warps = 0;
+    size_t smem_bytes = 0;
+    void* kernel = nullptr;
+    unsigned long long* inw = nullptr;     // epoch-tagged exact set, per warp
+    unsigned long long* gfilter = nullptr; // epoch-tagged lossy filter, per warp
+    uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
+};
+
+pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswState& H);
+pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params& p,
+                       const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
+                       int32_t* dists, pgb_query_stats* stats, cudaStream_t stream);
+void hnsw_release(HnswState& H);
+
+}  // namespace pgb

@@ -1,0 +1,44 @@
+// search_plan.h -- launch planning for the flat and HNSW search kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/pgb.h"
+#include "search_flat.cuh"
+
+namespace pgb {
+
+struct FlatPlanRequest {
+    uint32_t max_ls = 10;          // largest beam served by the launch
+    uint32_t deg_lim = 32;         // adjacency entries read per row
+    bool is_signed = true;
+    bool batched = false;
+    int warps_per_block = 0;       // 0: default (4)
+    int max_blocks_per_sm = 0;     // 0: as many as fit
+    uint32_t filter_smem_limit = 16384;   // bytes: filter in shared memory up to this
+    uint32_t visited_smem_limit = 8192;   // bytes: visited table in shared memory up to this
+    bool force_filter_placement = false;
+    bool filter_in_shared = true;
+    bool force_visited_placement = false;
+    bool visited_in_shared = true;
+};
+
+struct FlatPlan {
+    int ch = 1;
+    bool batched = false, is_signed = true, sfilt = true, svis = true;
+    FlatLayout L{};
+    uint32_t gfilter_words = 0, gvisited_words = 0;  // per warp, 0 when in shared memory
+    int warps_per_block = 4, blocks_per_sm = 1, blocks = 1;
+    uint64_t total_warps = 0;
+    size_t smem_bytes = 0;
+    void* kernel = nullptr;
+};
+
+int flat_chunks_for(uint32_t deg_lim);
+pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P);
+// A's table pointers must cover P.total_warps slices when the plan keeps them global
+pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream);
+
+}  // namespace pgb

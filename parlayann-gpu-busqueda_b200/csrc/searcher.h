@@ -1,0 +1,29 @@
+// searcher.h -- the searcher object behind pgb_searcher_*.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/pgb.h"
+#include "search_hnsw.h"
+#include "search_plan.h"
+
+struct pgb_searcher {
+    pgb_index* index = nullptr;
+    pgb_query_params params{};
+    uint32_t max_queries = 0;
+    pgb::FlatPlan flat{};
+    uint32_t* gfilter = nullptr;   // flat: per-warp filters when not in shared memory
+    uint32_t* gvisited = nullptr;  // flat: per-warp visited tables when not in shared
+    pgb::HnswState hnsw{};
+    // host-memory path staging
+    uint8_t* q_dev = nullptr;
+    uint32_t* ids_dev = nullptr;
+    int32_t* dists_dev = nullptr;
+    pgb_query_stats* stats_dev = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+namespace pgb {
+pgb_status cuda_status(cudaError_t e, const char* what);
+pgb_status check_params(const pgb_index* ix, const pgb_query_params* p);
+}  // namespace pgb

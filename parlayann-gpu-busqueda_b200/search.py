@@ -1,0 +1,223 @@
+"""Python host side over the C ABI: index, searcher (BuscadorGPU / BuscadorHnsw), builders.
+
+Mirrors the reference's search interface (reference cuda/busqueda.cuh:36-61,
+cuda/hnsw.h:65-86): a searcher is prepared for (graph, number of queries, config)
+(``preparar``), launched asynchronously on a stream (``lanzar``) and released
+(``liberar``). ConfigBusqueda{Ls, limite, k, cut} becomes QueryParams with ParlayANN's
+names {k, beam_size, cut, limit, degree_limit}. Errors raise PgbError (the reference
+exits the process instead).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native as N
+from .formats import Graph, Hnsw
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor."""
+    if a is None:
+        return 0
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())
+
+
+def _elem(dtype) -> int:
+    return N.PGB_INT8 if np.dtype(dtype) == np.int8 else N.PGB_UINT8
+
+
+@dataclass
+class QueryParams:
+    """ParlayANN QueryParams; defaults are the reference's ConfigBusqueda
+    (Ls=10, no visit limit, k=10, cut=1.35)."""
+    k: int = 10
+    beam_size: int = 10
+    cut: float = 1.35
+    limit: int = 0                 # <= 0: n
+    degree_limit: int = 0          # 0: graph max degree
+    exclude_query_id: bool = True  # ParlayANN wrapper's `a == p.id()` quirk (flat graphs)
+    query_id_base: int = 0
+
+    def to_c(self) -> N.QueryParams:
+        return N.QueryParams(self.k, self.beam_size, float(self.cut), int(self.limit),
+                             self.degree_limit, 1 if self.exclude_query_id else 0,
+                             self.query_id_base, 0)
+
+
+class Index:
+    """Device-resident index (vectors + graph). Read-only after creation."""
+
+    def __init__(self, handle: int, dtype):
+        self._h = C.c_void_p(handle)
+        self.dtype = np.dtype(dtype)
+        info = N.IndexInfo()
+        N.check(N.lib.pgb_index_get_info(self._h, C.byref(info)))
+        self.info = info
+
+    @classmethod
+    def flat(cls, vectors: np.ndarray, graph: Graph, device: int = 0) -> "Index":
+        v = np.ascontiguousarray(vectors)
+        deg = np.ascontiguousarray(graph.degrees, dtype=np.uint32)
+        edges = np.ascontiguousarray(graph.edges, dtype=np.uint32)
+        h = C.c_void_p()
+        N.check(N.lib.pgb_index_create_flat(device, _ptr(v), v.shape[0], v.shape[1],
+                                            _elem(v.dtype), _ptr(deg),
+                                            _ptr(edges) if edges.size else 0, C.byref(h)))
+        return cls(h.value, v.dtype)
+
+    @classmethod
+    def hnsw(cls, vectors: np.ndarray, h: Hnsw, device: int = 0) -> "Index":
+        v = np.ascontiguousarray(vectors)
+        arrs = [np.ascontiguousarray(a, dtype=np.uint32)
+                for a in (h.levels, h.node_point, h.list_sizes, h.ids, h.entries)]
+        out = C.c_void_p()
+        N.check(N.lib.pgb_index_create_hnsw(device, _ptr(v), v.shape[0], v.shape[1],
+                                            _elem(v.dtype), h.n, *[_ptr(a) for a in arrs[:4]],
+                                            _ptr(arrs[4]), len(arrs[4]), C.byref(out)))
+        return cls(out.value, v.dtype)
+
+    @classmethod
+    def load_flat(cls, vectors_path: str, graph_path: str, dtype=np.int8, device: int = 0):
+        h = C.c_void_p()
+        N.check(N.lib.pgb_index_load_flat(device, vectors_path.encode(), _elem(dtype),
+                                          graph_path.encode(), C.byref(h)))
+        return cls(h.value, dtype)
+
+    @classmethod
+    def load_hnsw(cls, vectors_path: str, hnsw_path: str, dtype=np.int8, device: int = 0):
+        h = C.c_void_p()
+        N.check(N.lib.pgb_index_load_hnsw(device, vectors_path.encode(), _elem(dtype),
+                                          hnsw_path.encode(), C.byref(h)))
+        return cls(h.value, dtype)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            N.lib.pgb_index_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Searcher:
+    """BuscadorGPU / BuscadorHnsw: prepare once for (index, max queries, params)."""
+
+    def __init__(self, index: Index, max_queries: int, params: QueryParams):
+        self.index, self.params, self.max_queries = index, params, max_queries
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        N.check(N.lib.pgb_searcher_create(index.handle, max_queries, C.byref(self._cp),
+                                          C.byref(h)))
+        self._h = h
+
+    def lanzar(self, queries, ids, dists, stats=None, stream: int = 0, query_stride=None):
+        """Asynchronous search of device queries into device outputs (torch tensors or
+        raw pointers); ``stream`` is a cudaStream_t value (0 = default stream)."""
+        nq = queries.shape[0]
+        stride = query_stride or (queries.stride(0) if hasattr(queries, "stride") else queries.shape[1])
+        N.check(N.lib.pgb_searcher_search(self._h, _ptr(queries), nq, stride, _ptr(ids),
+                                          _ptr(dists), _ptr(stats), C.c_void_p(stream)))
+
+    def search_device(self, queries, stream: int = 0):
+        """torch CUDA uint8/int8 queries [nq, dim] -> (ids, dists, stats) torch tensors."""
+        import torch
+        nq, k = queries.shape[0], self.params.k
+        ids = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        dists = torch.empty((nq, k), dtype=torch.int32, device=queries.device)
+        stats = torch.empty((nq, 4), dtype=torch.int32, device=queries.device)
+        self.lanzar(queries, ids, dists, stats, stream)
+        return ids, dists, stats
+
+    def search(self, queries: np.ndarray):
+        """Host queries -> host (ids uint32 [nq,k], dists int32 [nq,k], stats int32 [nq,4]),
+        synchronous (query upload, search, result download)."""
+        q = np.ascontiguousarray(queries)
+        nq, k = q.shape[0], self.params.k
+        ids = np.empty((nq, k), dtype=np.uint32)
+        dists = np.empty((nq, k), dtype=np.int32)
+        stats = np.empty((nq, 4), dtype=np.int32)
+        N.check(N.lib.pgb_searcher_search_host(self._h, _ptr(q), nq, q.shape[1], _ptr(ids),
+                                               _ptr(dists), _ptr(stats)))
+        return ids, dists, stats
+
+    def liberar(self):
+        if self._h:
+            N.lib.pgb_searcher_destroy(self._h)
+            self._h = C.c_void_p()
+
+    close = liberar
+
+    def __del__(self):
+        try:
+            self.liberar()
+        except Exception:
+            pass
+
+
+def recall(gt_ids: np.ndarray, gt_dists: np.ndarray, ids: np.ndarray, k: int) -> float:
+    """recall@k with distance ties (big-ann-benchmarks compute_recall_with_distance_ties;
+    reference cuda/evaluacion.cpp:184-208)."""
+    gi = np.ascontiguousarray(gt_ids, dtype=np.uint32)
+    gd = np.ascontiguousarray(gt_dists, dtype=np.float32)
+    ii = np.ascontiguousarray(ids[:, :k], dtype=np.uint32)
+    r = N.lib.pgb_recall(_ptr(gi), _ptr(gd), gi.shape[0], gi.shape[1], _ptr(ii), k)
+    if r < 0:
+        raise ValueError("recall: bad arguments")
+    return r
+
+
+# ---- builders (CPU, deterministic) ----------------------------------------------------
+def build_vamana(x: np.ndarray, R: int = 32, L: int = 64, alpha: float = 1.2, passes: int = 1,
+                 seed: int = 0, threads: int = 0) -> Graph:
+    x = np.ascontiguousarray(x)
+    deg = np.empty(x.shape[0], dtype=np.uint32)
+    adj = np.empty((x.shape[0], R), dtype=np.uint32)
+    N.check(N.lib.pgb_build_vamana(_ptr(x), x.shape[0], x.shape[1], _elem(x.dtype), R, L,
+                                   alpha, passes, seed, threads, _ptr(deg), _ptr(adj)))
+    return Graph.from_padded(deg, adj)
+
+
+def build_hcnng(x: np.ndarray, trees: int = 30, leaf: int = 1000, mst_deg: int = 3,
+                seed: int = 0, threads: int = 0) -> Graph:
+    x = np.ascontiguousarray(x)
+    slots = trees * mst_deg
+    deg = np.empty(x.shape[0], dtype=np.uint32)
+    adj = np.empty((x.shape[0], slots), dtype=np.uint32)
+    N.check(N.lib.pgb_build_hcnng(_ptr(x), x.shape[0], x.shape[1], _elem(x.dtype), trees, leaf,
+                                  mst_deg, seed, threads, _ptr(deg), _ptr(adj)))
+    return Graph.from_padded(deg, adj)
+
+
+def build_nndescent(x: np.ndarray, K: int = 40, init_trees: int = 10, leaf: int = 1000,
+                    alpha: float = 1.2, delta: float = 0.05, max_iters: int = 8, seed: int = 0,
+                    threads: int = 0) -> Graph:
+    x = np.ascontiguousarray(x)
+    deg = np.empty(x.shape[0], dtype=np.uint32)
+    adj = np.empty((x.shape[0], K), dtype=np.uint32)
+    N.check(N.lib.pgb_build_nndescent(_ptr(x), x.shape[0], x.shape[1], _elem(x.dtype), K,
+                                      init_trees, leaf, alpha, delta, max_iters, seed, threads,
+                                      _ptr(deg), _ptr(adj)))
+    return Graph.from_padded(deg, adj)
+
+
+def build_hnsw(x: np.ndarray, path: str, M: int = 32, ef_construction: int = 128,
+               ml: float = 0.36, alpha: float = 0.83, seed: int = 0, threads: int = 0) -> None:
+    x = np.ascontiguousarray(x)
+    N.check(N.lib.pgb_build_hnsw(_ptr(x), x.shape[0], x.shape[1], _elem(x.dtype), M,
+                                 ef_construction, ml, alpha, seed, threads, path.encode()))
+
+
+def device_available() -> bool:
+    return bool(N.lib.pgb_device_available())

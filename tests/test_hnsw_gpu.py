@@ -1,0 +1,28 @@
+"""Parity of the CUDA HNSW search with the oracle, through the C ABI."""
+import pytest
+
+from conftest import assert_same
+
+pytestmark = pytest.mark.gpu
+
+HNSW_CFGS = [(10, 0, 10), (50, 0, 10), (100, 0, 10), (50, 5, 10), (20, 0, 20), (150, 0, 10),
+             (300, 0, 10)]
+
+
+@pytest.mark.parametrize("name", ["hnsw", "ties_hnsw"])
+@pytest.mark.parametrize("cfg", HNSW_CFGS, ids=lambda c: "L%d_v%d_k%d" % c)
+def test_hnsw_matches_oracle(pgb, oracle, golden, gpu, name, cfg):
+    Ls, visit, k = cfg
+    base, queries = golden.vectors_for(name)
+    h = golden.hnsw[name]
+    index = pgb.Index.hnsw(base, h)
+    s = pgb.Searcher(index, len(queries), pgb.QueryParams(k=k, beam_size=Ls, limit=visit))
+    ids, dists, stats = s.search(queries)
+    s.liberar()
+    index.close()
+    oid, od, oc, oe, of = oracle.hnsw_search(base, h, queries, k, Ls, limit=visit)
+    assert_same("ids", ids, oid)
+    assert_same("dists", dists, od)
+    assert_same("comps", stats[:, 0], oc)
+    assert_same("expansions", stats[:, 1], oe)
+    assert_same("flags", stats[:, 2], of)

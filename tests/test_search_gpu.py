@@ -1,0 +1,42 @@
+"""Parity of the CUDA flat-graph search with the oracle (bit-exact ids, int32 distances,
+distance counts, expansions and flags), through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import assert_same
+
+pytestmark = pytest.mark.gpu
+
+FLAT_CFGS = [  # (Ls, visit, k, cut) -- the reference's (Ls, visit) configs at small scale
+    (10, 3, 10, 1.35), (10, 8, 10, 1.35), (10, 0, 10, 1.35), (20, 0, 10, 1.35),
+    (40, 0, 10, 1.35), (80, 0, 10, 1.35), (40, 0, 10, 0.9), (64, 0, 50, 1.35),
+    (150, 0, 10, 1.35), (300, 0, 10, 1.35),
+]
+
+
+def run_both(pgb, oracle, base, queries, graph, Ls, visit, k, cut, **kw):
+    index = pgb.Index.flat(base, graph)
+    p = pgb.QueryParams(k=k, beam_size=Ls, cut=cut, limit=visit, **kw)
+    s = pgb.Searcher(index, len(queries), p)
+    ids, dists, stats = s.search(queries)
+    s.liberar()
+    index.close()
+    o = oracle.flat_search(base, graph.degrees, graph.edges, queries, k, Ls, cut=cut, limit=visit,
+                           degree_limit=kw.get("degree_limit", 0),
+                           exclude_query_id=kw.get("exclude_query_id", True),
+                           query_id_base=kw.get("query_id_base", 0))
+    return (ids, dists, stats), o
+
+
+@pytest.mark.parametrize("graph_name", ["vamana", "hcnng", "nnd", "ties_vamana"])
+@pytest.mark.parametrize("cfg", FLAT_CFGS, ids=lambda c: "L%d_v%d_k%d_c%g" % c)
+def test_flat_matches_oracle(pgb, oracle, golden, gpu, graph_name, cfg):
+    Ls, visit, k, cut = cfg
+    base, queries = golden.vectors_for(graph_name)
+    (ids, dists, stats), (oid, od, oc, oe, of) = run_both(
+        pgb, oracle, base, queries, golden.graphs[graph_name], Ls, visit, k, cut)
+    assert_same("ids", ids, oid)
+    assert_same("dists", dists, od)
+    assert_same("comps", stats[:, 0], oc)
+    assert_same("expansions", stats[:, 1], oe)
+    assert_same("flags", stats[:, 2], of)
