@@ -1,0 +1,460 @@
+"""Benchmark: QPS at recall@10 = 0.90, batched vs plain warp-per-query kernel, on B200.
+
+Workload (one GPU): 1,000,000 int8 d=100 vectors (seeded Gaussian mixture standing in
+for MSSPACEV-1M), Vamana R=64 L=128 alpha=1.2, 29,316 queries, k=10. A step is one search
+of all queries. The operating point is the smallest beam of the 18-value sweep whose
+recall@10 (with distance ties, against exact GPU brute force) is >= 0.90.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank searches its own 29,316 queries against its own replica of
+the index (weak scaling, no collective on the data path); the step time is the max over
+ranks. ``--impl reference`` times the CPU restatement of the reference's search
+(oracle/, all host threads) on the same workload; rank 0 alone runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import __graft_entry__ as ge  # noqa: E402
+
+N_BASE = 1_000_000
+N_QUERIES = 29_316
+K = 10
+R, L_BUILD, ALPHA = 64, 128, 1.2
+TARGET_RECALL = 0.90
+METRIC = "QPS @ recall@10=0.90, batched vs plain kernel, 1 B200; serving p50/p99 latency"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def data_dir():
+    d = os.environ.get("PGB_DATA", os.path.join(ROOT, "_data"))
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_workload(pgb, rank, barrier):
+    """Base vectors, this rank's queries and the Vamana graph (cached on disk)."""
+    from parlayann_gpu_busqueda_b200 import synthetic as syn
+    d = data_dir()
+    base_p = os.path.join(d, "c2_base.i8bin")
+    graph_p = os.path.join(d, f"c2_vamana_R{R}_L{L_BUILD}_a{ALPHA}.graph")
+    if rank == 0:
+        if not os.path.exists(base_p):
+            base = syn.LAW_C2.sample(N_BASE, 0, 0)
+            pgb.write_vectors(base_p + ".tmp", base)
+            os.replace(base_p + ".tmp", base_p)
+        if not os.path.exists(graph_p):
+            base = pgb.read_vectors(base_p)
+            t = time.time()
+            g = pgb.build_vamana(base, R=R, L=L_BUILD, alpha=ALPHA, seed=0)
+            log(f"built Vamana 1M in {time.time() - t:.1f} s")
+            pgb.write_graph(graph_p + ".tmp", g)
+            os.replace(graph_p + ".tmp", graph_p)
+    barrier()
+    base = pgb.read_vectors(base_p)
+    graph = pgb.read_graph(graph_p)
+    queries = syn.LAW_C2.sample(N_QUERIES, 0, 1 + rank)
+    return base, queries, graph
+
+
+def ground_truth(base, queries, rank, device):
+    from parlayann_gpu_busqueda_b200 import groundtruth, formats
+    p = os.path.join(data_dir(), f"c2_gt100_q{rank}.bin")
+    if os.path.exists(p):
+        return formats.read_gt(p)
+    ids, dists = groundtruth.knn_gpu(base, queries, 100, device)
+    formats.write_gt(p + f".tmp{rank}", ids, dists)
+    os.replace(p + f".tmp{rank}", p)
+    return ids, dists
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while active."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu, self.proc, self.file = gpu_index, None, None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.file:
+            return None
+        self.file.flush()
+        rows = [r.split(", ") for r in open(self.file.name).read().strip().splitlines() if r]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        m = json.load(open(p))
+        return float(m["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_reference(args, rank):
+    """CPU restatement of the reference search (oracle) on the host cores."""
+    if rank != 0:
+        return
+    pgb = ge.load_package()
+    oracle = ge.load_oracle()
+    base, queries, graph = load_workload(pgb, 0, lambda: None)
+    gt_p = os.path.join(data_dir(), "c2_gt100_q0.bin")
+    Ls = int(os.environ.get("PGB_REF_LS", "0"))
+    from parlayann_gpu_busqueda_b200 import formats
+    if not Ls:
+        # same rule as our arm: smallest sweep beam reaching the target recall
+        from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
+        gi, gd = formats.read_gt(gt_p) if os.path.exists(gt_p) else (None, None)
+        Ls = 40
+        if gi is not None:
+            sample = slice(0, 2000)
+            for ls in LS_SWEEP:
+                ids = oracle.flat_search(base, graph.degrees, graph.edges, queries[sample], K, ls)[0]
+                if oracle.recall(gi[sample], gd[sample], ids, K) >= TARGET_RECALL:
+                    Ls = ls
+                    break
+    threads = os.cpu_count() or 1
+    # bounded sample: every step searches the first `sample` queries on all threads
+    sample = min(N_QUERIES, int(os.environ.get("PGB_REF_SAMPLE", "8192")))
+    q = np.ascontiguousarray(queries[:sample])
+    for _ in range(args.warmup):
+        oracle.flat_search(base, graph.degrees, graph.edges, q, K, Ls, threads=threads)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        oracle.flat_search(base, graph.degrees, graph.edges, q, K, Ls, threads=threads)
+        times.append(time.perf_counter() - t)
+    qps = sample * len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": "1M int8 d=100 Vamana R64 L128 a1.2, k=10", "Ls": Ls,
+                   "queries_per_step": sample},
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_profile(args, local):
+    """Launches only the search kernels (plain, then batched) on a small query set."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    base, queries, graph = load_workload(pgb, 0, lambda: None)
+    nq, Ls = args.profile_nq, args.profile_ls
+    index = pgb.Index.flat(base, graph, device=local)
+    q = torch.from_numpy(np.ascontiguousarray(queries[:nq]).view(np.uint8)).to(dev)
+    sp = torch.cuda.current_stream(dev).cuda_stream
+    s = pgb.Searcher(index, nq, pgb.QueryParams(k=K, beam_size=Ls))
+    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    d = torch.empty_like(ids)
+    st = torch.empty((nq, 4), dtype=torch.int32, device=dev)
+    b = pgb.Batch(index, nq, max_beam=Ls, max_k=K, warps_per_block=4, filter_placement=1,
+                  visited_placement=2)
+    b.plan(np.full(nq, Ls, np.uint32), np.full(nq, K, np.uint32))
+    for _ in range(args.warmup + args.steps):
+        s.lanzar(q, ids, d, st, sp)
+    for _ in range(args.warmup + args.steps):
+        b.search(q, ids, d, st, sp)
+    torch.cuda.synchronize(dev)
+    stn = st.cpu().numpy()
+    print(json.dumps({"profile": True, "nq": nq, "Ls": Ls,
+                      "comps": int(stn[:, 0].astype(np.int64).sum()),
+                      "expansions": int(stn[:, 1].astype(np.int64).sum()),
+                      "row_stride": (int(index.info.max_degree) + 31) // 32 * 32}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="small case for ncu: the 1M index, --profile-nq queries at --profile-ls, "
+                         "warm-up then --steps launches of each kernel, nothing else")
+    ap.add_argument("--profile-nq", type=int, default=8192)
+    ap.add_argument("--profile-ls", type=int, default=40)
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.profile:
+        run_profile(args, local)
+        return
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800),
+                                device_id=dev)
+        barrier = lambda: dist.barrier()  # noqa: E731
+    else:
+        barrier = lambda: None  # noqa: E731
+
+    pgb = ge.load_package()
+    from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
+    t0 = time.time()
+    base, queries, graph = load_workload(pgb, rank, barrier)
+    gt_ids, gt_d = ground_truth(base, queries, rank, local)
+    index = pgb.Index.flat(base, graph, device=local)
+    log(f"rank {rank}: setup {time.time() - t0:.1f} s, index {index.info.device_bytes / 2**20:.0f} MiB")
+    q_dev = torch.from_numpy(queries.view(np.uint8)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    # ---- operating point: smallest sweep beam with recall@10 >= 0.90 ---------------
+    sweep, Ls = [], None
+    for ls in LS_SWEEP:
+        s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=ls))
+        ids, dists, st = s.search_device(q_dev, sp)
+        torch.cuda.synchronize(dev)
+        rec = pgb.recall(gt_ids, gt_d, ids.cpu().numpy().view(np.uint32), K)
+        sweep.append([ls, round(rec, 5)])
+        s.liberar()
+        if rec >= TARGET_RECALL and Ls is None:
+            Ls = ls
+        if Ls is not None and ls >= 2 * Ls:
+            break
+    if Ls is None:
+        Ls = LS_SWEEP[-1]
+    recall_at = dict((a, b) for a, b in sweep)[Ls]
+
+    # L2 flush between timed steps (a write larger than the 126 MB L2)
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        ev = []
+        for _ in range(steps):
+            flush.fill_(1)
+            barrier()
+            torch.cuda.synchronize(dev)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            barrier()
+            ev.append(a.elapsed_time(b))
+        return ev
+
+    # ---- plain warp-per-query kernel (the drop-in) ----------------------------------
+    plain = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=Ls))
+    p_ids = torch.empty((N_QUERIES, K), dtype=torch.int32, device=dev)
+    p_d = torch.empty_like(p_ids)
+    p_st = torch.empty((N_QUERIES, 4), dtype=torch.int32, device=dev)
+    run_plain = lambda: plain.lanzar(q_dev, p_ids, p_d, p_st, sp)  # noqa: E731
+
+    # ---- batched persistent kernel: tuned, CUDA-graph captured -----------------------
+    batch = pgb.Batch(index, N_QUERIES, max_beam=Ls, max_k=K)
+    batch.plan(np.full(N_QUERIES, Ls, np.uint32), np.full(N_QUERIES, K, np.uint32))
+    b_ids, b_d, b_st = batch.outputs(dev)
+    tuned = batch.tune(q_dev, b_ids, b_d, b_st)
+    batch.capture(q_dev, b_ids, b_d, b_st)
+    run_batched = lambda: batch.replay(sp)  # noqa: E731
+
+    clk = ClockSampler(local).__enter__()
+    time.sleep(0.6)  # let the sampler come up before the timed region
+    t_plain = timed(run_plain, args.steps, args.warmup)
+    t_batch = timed(run_batched, args.steps, args.warmup)
+    identical = bool(torch.equal(p_ids, b_ids) and torch.equal(p_d, b_d))
+
+    # ---- end to end through the public host API (pinned host buffers) ---------------
+    q_host = torch.from_numpy(queries.view(np.uint8)).pin_memory()
+    e_ids = torch.empty((N_QUERIES, K), dtype=torch.int32).pin_memory()
+    e_d = torch.empty((N_QUERIES, K), dtype=torch.int32).pin_memory()
+    import ctypes as C
+    lib = pgb._native.lib
+
+    def run_e2e():
+        rc = lib.pgb_searcher_search_host(plain._h, q_host.data_ptr(), N_QUERIES, queries.shape[1],
+                                          e_ids.data_ptr(), e_d.data_ptr(), None)
+        pgb._native.check(rc)
+
+    for _ in range(args.warmup):
+        run_e2e()
+    e2e_t = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize(dev)
+        barrier()
+        t = time.perf_counter()
+        run_e2e()
+        e2e_t.append(time.perf_counter() - t)
+        barrier()
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
+    e2e_ok = bool(np.array_equal(e_ids.numpy(), p_ids.cpu().numpy()))
+
+    # ---- max over ranks ---------------------------------------------------------------
+    def worst(xs):
+        t = torch.tensor([sum(xs)], dtype=torch.float64, device=dev)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    tp_ms, tb_ms, te_s = worst(t_plain), worst(t_batch), worst(e2e_t)
+    total_q = N_QUERIES * world * args.steps
+    qps_plain = total_q / (tp_ms / 1e3)
+    qps_batch = total_q / (tb_ms / 1e3)
+    qps_e2e = total_q / te_s
+
+    # ---- roofline of the plain kernel: algorithmic gather bytes per launch ----------
+    st = p_st.cpu().numpy()
+    G = int(index.info.max_degree)
+    gs = (G + 31) // 32 * 32
+    bytes_launch = float(128 * st[:, 0].astype(np.int64).sum() + 4 * gs * st[:, 1].astype(np.int64).sum())
+    avg_plain_s = (sum(t_plain) / len(t_plain)) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_launch / avg_plain_s / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "flat_plain_c2_traffic.json")
+    if os.path.exists(tp):
+        tr = json.load(open(tp))
+        if tr.get("Ls") == Ls and tr.get("nq") == N_QUERIES:
+            traffic = tr.get("dram_bytes_per_launch")
+
+    cpu_baseline = None
+    if rank == 0 and not args.no_cpu_baseline:
+        oracle = ge.load_oracle()
+        sample = 8192
+        qs = np.ascontiguousarray(queries[:sample])
+        threads = os.cpu_count() or 1
+        oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls, threads=threads)
+        ts = []
+        for _ in range(2):
+            t = time.perf_counter()
+            oid = oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls, threads=threads)[0]
+            ts.append(time.perf_counter() - t)
+        assert np.array_equal(oid, p_ids[:sample].cpu().numpy().view(np.uint32)), \
+            "CUDA result differs from the CPU restatement"
+        cpu_baseline = {"value": sample / min(ts), "unit": "queries/s", "cores": threads,
+                        "kind": "port",
+                        "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}, best of 2"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": qps_batch,
+            "unit": "queries/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": tb_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "int8",
+            "data": "synthetic",
+            "config": {
+                "workload": "1M int8 d=100 Gaussian mixture (1024 centres, sigma 10, 30% zeros), "
+                            "Vamana R64 L128 alpha1.2, 29316 queries per GPU, k=10",
+                "Ls": Ls, "recall_at_10": recall_at, "sweep_recall": sweep,
+                "parallelism": f"queries sharded, index replicated x{world}",
+                "l2": "flushed (512 MiB write) before every timed step; index 384 MB > L2",
+                "plain_qps": qps_plain, "batched_qps": qps_batch,
+                "batched_over_plain": qps_batch / qps_plain,
+                "batched_config": tuned, "identical_neighbours": identical,
+            },
+            "e2e": {"value": qps_e2e, "unit": "queries/s",
+                    "h2d_bytes_per_step": int(queries.nbytes),
+                    "d2h_bytes_per_step": int(2 * 4 * N_QUERIES * K),
+                    "identical_neighbours": e2e_ok},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": peak_kind,
+                         "kernel": "flat_plain_kernel", "bytes_per_launch": bytes_launch,
+                         "avg_launch_ms": avg_plain_s * 1e3,
+                         "comps_per_query": float(st[:, 0].mean()),
+                         "expansions_per_query": float(st[:, 1].mean())},
+            "cpu_baseline": cpu_baseline,
+            "clocks": clocks,
+            "gpu_launches": 3 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    plain.liberar()
+    batch.close()
+    index.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -149,6 +149,50 @@ pgb_status pgb_searcher_search_host(pgb_searcher* s, const void* queries, uint32
 /* liberar */
 pgb_status pgb_searcher_destroy(pgb_searcher* s);
 
+/* ---- batched persistent form (no counterpart in the reference) -----------------------
+ * One persistent launch serves queries of different beam sizes and k: warps pull the next
+ * query from a device counter over a longest-beam-first order, so a long beam never holds
+ * a block. Neighbours are identical to pgb_searcher_search with the same per-query params.
+ * Outputs use a row stride of max_k; row q holds k_q entries then padding. */
+typedef struct pgb_batch_options {
+    uint32_t max_queries;
+    uint32_t max_beam;          /* largest Ls planned                                   */
+    uint32_t max_k;             /* largest k planned; output row stride                 */
+    double cut;
+    int64_t limit;              /* <= 0: n                                              */
+    uint32_t degree_limit;      /* 0: graph max degree                                  */
+    uint32_t exclude_query_id;
+    uint32_t query_id_base;
+    uint32_t warps_per_block;   /* 0: default / tuned                                   */
+    uint32_t filter_placement;  /* 0 auto, 1 shared memory, 2 global memory             */
+    uint32_t visited_placement; /* 0 auto, 1 shared memory, 2 global memory             */
+} pgb_batch_options;
+
+typedef struct pgb_batch_config {
+    uint32_t warps_per_block, blocks, filter_in_shared, visited_in_shared;
+    uint32_t shared_bytes_per_warp;
+    float tuned_ms;             /* time of the chosen config in the last tune (0: untuned) */
+} pgb_batch_config;
+
+pgb_status pgb_batch_create(pgb_index* index, const pgb_batch_options* opt, pgb_batch** out);
+/* Host step: per-query beam sizes and k (host arrays of nq); uploads the work order. */
+pgb_status pgb_batch_plan(pgb_batch* b, const uint32_t* beam_sizes, const uint32_t* ks,
+                          uint32_t nq);
+/* Device step: one launch over the planned queries (device pointers); capturable. */
+pgb_status pgb_batch_search(pgb_batch* b, const void* queries, uint32_t query_stride,
+                            uint32_t* ids, int32_t* dists, pgb_query_stats* stats,
+                            void* stream);
+/* Autotuner: times the candidate launch shapes and table placements on the planned
+ * queries (outputs are overwritten) and keeps the fastest. Synchronous. */
+pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t query_stride,
+                          uint32_t* ids, int32_t* dists, pgb_query_stats* stats);
+pgb_status pgb_batch_get_config(const pgb_batch* b, pgb_batch_config* out);
+/* CUDA graph of (counter reset + launch) for these buffers; replay on any stream. */
+pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t query_stride,
+                             uint32_t* ids, int32_t* dists, pgb_query_stats* stats);
+pgb_status pgb_batch_replay(pgb_batch* b, void* stream);
+pgb_status pgb_batch_destroy(pgb_batch* b);
+
 /* ---- evaluation ---------------------------------------------------------------- */
 /* recall@k with distance ties (big-ann-benchmarks compute_recall_with_distance_ties). */
 double pgb_recall(const uint32_t* gt_ids, const float* gt_dists, uint32_t nq, uint32_t gt_k,

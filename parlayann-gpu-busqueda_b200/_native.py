@@ -95,3 +95,27 @@ def check(status: int) -> None:
     if status != PGB_OK:
         msg = lib.pgb_last_error()
         raise PgbError(status, msg.decode() if msg else "")
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("max_queries", C.c_uint32), ("max_beam", C.c_uint32), ("max_k", C.c_uint32),
+                ("cut", C.c_double), ("limit", C.c_int64), ("degree_limit", C.c_uint32),
+                ("exclude_query_id", C.c_uint32), ("query_id_base", C.c_uint32),
+                ("warps_per_block", C.c_uint32), ("filter_placement", C.c_uint32),
+                ("visited_placement", C.c_uint32)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("warps_per_block", C.c_uint32), ("blocks", C.c_uint32),
+                ("filter_in_shared", C.c_uint32), ("visited_in_shared", C.c_uint32),
+                ("shared_bytes_per_warp", C.c_uint32), ("tuned_ms", C.c_float)]
+
+
+_sig("pgb_batch_create", C.c_int, vp, C.POINTER(BatchOptions), C.POINTER(vp))
+_sig("pgb_batch_plan", C.c_int, vp, vp, vp, u32)
+_sig("pgb_batch_search", C.c_int, vp, vp, u32, vp, vp, vp, vp)
+_sig("pgb_batch_tune", C.c_int, vp, vp, u32, vp, vp, vp)
+_sig("pgb_batch_get_config", C.c_int, vp, C.POINTER(BatchConfig))
+_sig("pgb_batch_capture", C.c_int, vp, vp, u32, vp, vp, vp)
+_sig("pgb_batch_replay", C.c_int, vp, vp)
+_sig("pgb_batch_destroy", C.c_int, vp)

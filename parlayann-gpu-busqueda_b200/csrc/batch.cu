@@ -1,0 +1,324 @@
+// batch.cu -- pgb_batch_*: the batched persistent form of the flat-graph search.
+//
+// plan   : host step, per-query (Ls, k) -> longest-beam-first work order on the device
+// search : cudaMemsetAsync(counter) + one persistent launch (capturable)
+// tune   : times candidate (warps per block, filter / visited placement) on the planned
+//          queries and keeps the fastest; every candidate returns identical neighbours,
+//          because all of them run the same per-query code (flat_query)
+#include <algorithm>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "errors.h"
+#include "index.h"
+#include "search_plan.h"
+#include "searcher.h"
+
+struct pgb_batch {
+    pgb_index* index = nullptr;
+    pgb_batch_options opt{};
+    pgb::FlatPlan plan{};
+    float tuned_ms = 0.f;
+    uint32_t* gfilter = nullptr;
+    uint64_t gfilter_words = 0;   // allocated words
+    uint32_t* gvisited = nullptr;
+    uint64_t gvisited_words = 0;
+    uint32_t* d_ls = nullptr;
+    uint32_t* d_k = nullptr;
+    uint32_t* d_order = nullptr;
+    uint32_t* d_queue = nullptr;
+    uint32_t nq = 0;
+    uint32_t max_ls_planned = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+};
+
+namespace pgb {
+namespace {
+
+pgb_status make_plan(pgb_batch* b, int wpb, int filter_pl, int visited_pl, FlatPlan& P) {
+    const pgb_index* ix = b->index;
+    FlatPlanRequest rq;
+    rq.max_ls = b->opt.max_beam;
+    rq.deg_lim = b->opt.degree_limit ? std::min(b->opt.degree_limit, ix->G) : ix->G;
+    rq.is_signed = ix->elem == PGB_INT8;
+    rq.batched = true;
+    rq.warps_per_block = wpb;
+    if (filter_pl) {
+        rq.force_filter_placement = true;
+        rq.filter_in_shared = filter_pl == 1;
+    }
+    if (visited_pl) {
+        rq.force_visited_placement = true;
+        rq.visited_in_shared = visited_pl == 1;
+    }
+    return plan_flat(rq, P);
+}
+
+// scratch for the plan's global tables (grown, never shrunk)
+pgb_status ensure_scratch(pgb_batch* b, const FlatPlan& P) {
+    const uint64_t fw = (uint64_t)P.gfilter_words * P.total_warps;
+    const uint64_t vw = (uint64_t)P.gvisited_words * P.total_warps;
+    pgb_status s;
+    if (fw > b->gfilter_words) {
+        cudaFree(b->gfilter);
+        b->gfilter = nullptr;
+        b->gfilter_words = 0;
+        if ((s = cuda_status(cudaMalloc(&b->gfilter, 4 * fw), "batch filter scratch")) != PGB_OK) return s;
+        b->gfilter_words = fw;
+    }
+    if (vw > b->gvisited_words) {
+        cudaFree(b->gvisited);
+        b->gvisited = nullptr;
+        b->gvisited_words = 0;
+        if ((s = cuda_status(cudaMalloc(&b->gvisited, 4 * vw), "batch visited scratch")) != PGB_OK) return s;
+        b->gvisited_words = vw;
+    }
+    return PGB_OK;
+}
+
+void drop_graph(pgb_batch* b) {
+    if (b->graph_exec) cudaGraphExecDestroy(b->graph_exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph_exec = nullptr;
+    b->graph = nullptr;
+}
+
+pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_t qstride,
+                   uint32_t* ids, int32_t* dists, pgb_query_stats* stats, cudaStream_t st) {
+    const pgb_index* ix = b->index;
+    pgb_status s = cuda_status(cudaMemsetAsync(b->d_queue, 0, sizeof(uint32_t), st), "queue reset");
+    if (s != PGB_OK) return s;
+    FlatArgs A{};
+    A.rows = ix->rows;
+    A.adj = ix->adj;
+    A.n = ix->n;
+    A.gs = ix->gs;
+    A.deg_lim = b->opt.degree_limit ? std::min(b->opt.degree_limit, ix->G) : ix->G;
+    A.dim = ix->dim;
+    A.start = 0;
+    A.queries = (const uint8_t*)queries;
+    A.nq = b->nq;
+    A.qstride = qstride;
+    A.cut = b->opt.cut;
+    A.limit = b->opt.limit <= 0 ? (int64_t)ix->n : b->opt.limit;
+    A.excl = b->opt.exclude_query_id ? 1u : 0u;
+    A.qbase = b->opt.query_id_base;
+    A.ls_arr = b->d_ls;
+    A.k_arr = b->d_k;
+    A.order = b->d_order;
+    A.out_stride = b->opt.max_k;
+    A.ids = ids;
+    A.dists = dists;
+    A.stats = stats;
+    A.gfilter = P.gfilter_words ? b->gfilter : nullptr;
+    A.gvisited = P.gvisited_words ? b->gvisited : nullptr;
+    A.queue = b->d_queue;
+    return launch_flat(P, A, st);
+}
+
+pgb_status check_call(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
+                      int32_t* dists) {
+    if (!b) return fail(PGB_ERR_BAD_ARG, "null batch");
+    if (b->nq == 0) return fail(PGB_ERR_BAD_ARG, "batch has no planned queries");
+    if (!queries || !ids || !dists) return fail(PGB_ERR_BAD_ARG, "null queries or outputs");
+    if (qstride < b->index->dim) return fail(PGB_ERR_BAD_ARG, "query_stride below dim");
+    return PGB_OK;
+}
+
+}  // namespace
+}  // namespace pgb
+
+using namespace pgb;
+
+extern "C" {
+
+pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_batch** out) {
+    if (!out) return fail(PGB_ERR_BAD_ARG, "null output handle");
+    *out = nullptr;
+    if (!ix || !opt) return fail(PGB_ERR_BAD_ARG, "null index or options");
+    if (ix->is_hnsw) return fail(PGB_ERR_BAD_ARG, "the batched form serves flat graphs");
+    if (opt->max_queries == 0 || opt->max_beam == 0 || opt->max_beam > PGB_MAX_BEAM ||
+        opt->max_k == 0 || opt->max_k > PGB_MAX_K || !(opt->cut > 0))
+        return fail(PGB_ERR_BAD_ARG, "bad max_queries / max_beam / max_k / cut");
+    if (opt->warps_per_block > 8 || opt->filter_placement > 2 || opt->visited_placement > 2)
+        return fail(PGB_ERR_BAD_ARG, "bad launch shape or placement option");
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    pgb_batch* b = new pgb_batch();
+    b->index = ix;
+    b->opt = *opt;
+    pgb_status s;
+    const size_t nq = opt->max_queries;
+    if ((s = make_plan(b, (int)opt->warps_per_block, (int)opt->filter_placement,
+                       (int)opt->visited_placement, b->plan)) != PGB_OK ||
+        (s = ensure_scratch(b, b->plan)) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->d_ls, 4 * nq), "batch arrays")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->d_k, 4 * nq), "batch arrays")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->d_order, 4 * nq), "batch arrays")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->d_queue, 4), "batch counter")) != PGB_OK) {
+        pgb_batch_destroy(b);
+        return s;
+    }
+    *out = b;
+    return PGB_OK;
+}
+
+pgb_status pgb_batch_plan(pgb_batch* b, const uint32_t* beam_sizes, const uint32_t* ks,
+                          uint32_t nq) {
+    if (!b || !beam_sizes || !ks) return fail(PGB_ERR_BAD_ARG, "null argument");
+    if (nq == 0 || nq > b->opt.max_queries) return fail(PGB_ERR_BAD_ARG, "nq outside 1..max_queries");
+    uint32_t mx = 0;
+    for (uint32_t i = 0; i < nq; i++) {
+        if (beam_sizes[i] == 0 || beam_sizes[i] > b->opt.max_beam)
+            return fail(PGB_ERR_BAD_ARG, "beam size outside 1..max_beam");
+        if (ks[i] == 0 || ks[i] > b->opt.max_k) return fail(PGB_ERR_BAD_ARG, "k outside 1..max_k");
+        mx = std::max(mx, beam_sizes[i]);
+    }
+    DeviceGuard guard(b->index->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    // longest beam first (stable), so the longest queries start before the short ones
+    std::vector<uint32_t> order(nq);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t c) { return beam_sizes[a] > beam_sizes[c]; });
+    pgb_status s;
+    if ((s = cuda_status(cudaMemcpy(b->d_ls, beam_sizes, 4ull * nq, cudaMemcpyHostToDevice), "plan upload")) != PGB_OK ||
+        (s = cuda_status(cudaMemcpy(b->d_k, ks, 4ull * nq, cudaMemcpyHostToDevice), "plan upload")) != PGB_OK ||
+        (s = cuda_status(cudaMemcpy(b->d_order, order.data(), 4ull * nq, cudaMemcpyHostToDevice), "plan upload")) != PGB_OK)
+        return s;
+    b->nq = nq;
+    b->max_ls_planned = mx;
+    drop_graph(b);
+    return PGB_OK;
+}
+
+pgb_status pgb_batch_search(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
+                            int32_t* dists, pgb_query_stats* stats, void* stream) {
+    pgb_status s = check_call(b, queries, qstride, ids, dists);
+    if (s != PGB_OK) return s;
+    DeviceGuard guard(b->index->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    return enqueue(b, b->plan, queries, qstride, ids, dists, stats, (cudaStream_t)stream);
+}
+
+pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
+                          int32_t* dists, pgb_query_stats* stats) {
+    pgb_status s = check_call(b, queries, qstride, ids, dists);
+    if (s != PGB_OK) return s;
+    DeviceGuard guard(b->index->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    cudaStream_t st;
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "tune stream")) != PGB_OK)
+        return s;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int wpbs[] = {2, 4, 8};
+    const int fpls[] = {1, 2};
+    const int vpls[] = {1, 2};
+    float best = 1e30f;
+    FlatPlan best_plan = b->plan;
+    for (int wpb : wpbs)
+        for (int fp : fpls)
+            for (int vp : vpls) {
+                if (b->opt.warps_per_block && (int)b->opt.warps_per_block != wpb) continue;
+                if (b->opt.filter_placement && (int)b->opt.filter_placement != fp) continue;
+                if (b->opt.visited_placement && (int)b->opt.visited_placement != vp) continue;
+                FlatPlan P;
+                if (make_plan(b, wpb, fp, vp, P) != PGB_OK) continue;  // does not fit
+                if (P.warps_per_block != wpb) continue;
+                if (ensure_scratch(b, P) != PGB_OK) continue;
+                float ms = 0.f, t = 0.f;
+                bool ok = enqueue(b, P, queries, qstride, ids, dists, stats, st) == PGB_OK;  // warm
+                for (int r = 0; r < 2 && ok; r++) {
+                    cudaEventRecord(e0, st);
+                    ok = enqueue(b, P, queries, qstride, ids, dists, stats, st) == PGB_OK;
+                    cudaEventRecord(e1, st);
+                    ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+                    cudaEventElapsedTime(&t, e0, e1);
+                    ms += t;
+                }
+                if (ok && ms / 2 < best) {
+                    best = ms / 2;
+                    best_plan = P;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaError_t e = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) return cuda_status(e, "tune");
+    if (best >= 1e30f) return fail(PGB_ERR_CUDA, "no candidate configuration ran");
+    b->plan = best_plan;
+    b->tuned_ms = best;
+    drop_graph(b);
+    return PGB_OK;
+}
+
+pgb_status pgb_batch_get_config(const pgb_batch* b, pgb_batch_config* out) {
+    if (!b || !out) return fail(PGB_ERR_BAD_ARG, "null argument");
+    out->warps_per_block = (uint32_t)b->plan.warps_per_block;
+    out->blocks = (uint32_t)b->plan.blocks;
+    out->filter_in_shared = b->plan.sfilt ? 1u : 0u;
+    out->visited_in_shared = b->plan.svis ? 1u : 0u;
+    out->shared_bytes_per_warp = b->plan.L.bytes;
+    out->tuned_ms = b->tuned_ms;
+    return PGB_OK;
+}
+
+pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
+                             int32_t* dists, pgb_query_stats* stats) {
+    pgb_status s = check_call(b, queries, qstride, ids, dists);
+    if (s != PGB_OK) return s;
+    DeviceGuard guard(b->index->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    drop_graph(b);
+    cudaStream_t st;
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "capture stream")) != PGB_OK)
+        return s;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        pgb_status ls = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(st, &g);
+        if (ls != PGB_OK) {
+            if (g) cudaGraphDestroy(g);
+            cudaStreamDestroy(st);
+            return ls;
+        }
+        if (e == cudaSuccess) {
+            b->graph = g;
+            e = cudaGraphInstantiate(&b->graph_exec, g, 0);
+        }
+    }
+    cudaStreamDestroy(st);
+    if (e != cudaSuccess) {
+        drop_graph(b);
+        return cuda_status(e, "graph capture");
+    }
+    return PGB_OK;
+}
+
+pgb_status pgb_batch_replay(pgb_batch* b, void* stream) {
+    if (!b || !b->graph_exec) return fail(PGB_ERR_BAD_ARG, "no captured graph");
+    DeviceGuard guard(b->index->device);
+    return cuda_status(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream), "graph launch");
+}
+
+pgb_status pgb_batch_destroy(pgb_batch* b) {
+    if (!b) return PGB_OK;
+    DeviceGuard guard(b->index ? b->index->device : 0);
+    drop_graph(b);
+    cudaFree(b->gfilter);
+    cudaFree(b->gvisited);
+    cudaFree(b->d_ls);
+    cudaFree(b->d_k);
+    cudaFree(b->d_order);
+    cudaFree(b->d_queue);
+    delete b;
+    return PGB_OK;
+}
+
+}  // extern "C"

@@ -221,3 +221,75 @@ def build_hnsw(x: np.ndarray, path: str, M: int = 32, ef_construction: int = 128
 
 def device_available() -> bool:
     return bool(N.lib.pgb_device_available())
+
+
+class Batch:
+    """Batched persistent form: one launch over queries with per-query (Ls, k).
+
+    plan() is the host step (longest beam first work order); search()/replay() are
+    device-only and return the same neighbours as Searcher with the same params.
+    Output rows have stride max_k."""
+
+    def __init__(self, index: Index, max_queries: int, max_beam: int, max_k: int,
+                 cut: float = 1.35, limit: int = 0, degree_limit: int = 0,
+                 exclude_query_id: bool = True, query_id_base: int = 0,
+                 warps_per_block: int = 0, filter_placement: int = 0, visited_placement: int = 0):
+        self.index, self.max_k = index, max_k
+        self._opt = N.BatchOptions(max_queries, max_beam, max_k, float(cut), int(limit),
+                                   degree_limit, 1 if exclude_query_id else 0, query_id_base,
+                                   warps_per_block, filter_placement, visited_placement)
+        h = C.c_void_p()
+        N.check(N.lib.pgb_batch_create(index.handle, C.byref(self._opt), C.byref(h)))
+        self._h = h
+        self.nq = 0
+
+    def plan(self, beam_sizes, ks):
+        ls = np.ascontiguousarray(beam_sizes, dtype=np.uint32)
+        kk = np.ascontiguousarray(ks, dtype=np.uint32)
+        assert ls.shape == kk.shape
+        N.check(N.lib.pgb_batch_plan(self._h, _ptr(ls), _ptr(kk), ls.shape[0]))
+        self.nq = ls.shape[0]
+
+    def _args(self, queries, ids, dists, stats):
+        stride = queries.stride(0) if hasattr(queries, "stride") else queries.shape[1]
+        return _ptr(queries), stride, _ptr(ids), _ptr(dists), _ptr(stats)
+
+    def search(self, queries, ids, dists, stats=None, stream: int = 0):
+        q, st, i, d, s = self._args(queries, ids, dists, stats)
+        N.check(N.lib.pgb_batch_search(self._h, q, st, i, d, s, C.c_void_p(stream)))
+
+    def tune(self, queries, ids, dists, stats=None):
+        q, st, i, d, s = self._args(queries, ids, dists, stats)
+        N.check(N.lib.pgb_batch_tune(self._h, q, st, i, d, s))
+        return self.config()
+
+    def config(self) -> dict:
+        c = N.BatchConfig()
+        N.check(N.lib.pgb_batch_get_config(self._h, C.byref(c)))
+        return {f: getattr(c, f) for f, _ in N.BatchConfig._fields_}
+
+    def capture(self, queries, ids, dists, stats=None):
+        q, st, i, d, s = self._args(queries, ids, dists, stats)
+        N.check(N.lib.pgb_batch_capture(self._h, q, st, i, d, s))
+
+    def replay(self, stream: int = 0):
+        N.check(N.lib.pgb_batch_replay(self._h, C.c_void_p(stream)))
+
+    def outputs(self, device):
+        """Device output buffers (torch) of the right shape for this batch."""
+        import torch
+        ids = torch.empty((self.nq, self.max_k), dtype=torch.int32, device=device)
+        dists = torch.empty((self.nq, self.max_k), dtype=torch.int32, device=device)
+        stats = torch.empty((self.nq, 4), dtype=torch.int32, device=device)
+        return ids, dists, stats
+
+    def close(self):
+        if self._h:
+            N.lib.pgb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -28,11 +28,17 @@ class MixtureLaw:
         return np.clip(np.rint(x), lo, hi).astype(np.int8 if self.signed else np.uint8)
 
     def sample(self, n: int, seed: int, stream: int, chunk: int = 1 << 20) -> np.ndarray:
+        """stream 0: base points; 1: queries; s >= 2: further independent query sets."""
         ss = np.random.SeedSequence(seed)
         c_seq, b_seq, q_seq = ss.spawn(3)
         centers = np.random.Generator(np.random.PCG64(c_seq)).uniform(
             self.center_lo, self.center_hi, size=(self.n_centers, self.dim)).astype(np.float32)
-        seq = b_seq if stream == 0 else q_seq
+        if stream == 0:
+            seq = b_seq
+        elif stream == 1:
+            seq = q_seq
+        else:
+            seq = np.random.SeedSequence(seed, spawn_key=(1000 + stream,))
         rng = np.random.Generator(np.random.PCG64(seq))
         out = np.empty((n, self.dim), dtype=np.int8 if self.signed else np.uint8)
         for s in range(0, n, chunk):

@@ -1,0 +1,88 @@
+"""The batched persistent form returns, query by query, the oracle's answer for that
+query's own (Ls, k) -- whatever launch shape or table placement the tuner picks."""
+import numpy as np
+import pytest
+
+from conftest import assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_rows(oracle, base, graph, queries, ls, ks, max_k, **kw):
+    ids = np.full((len(queries), max_k), 0xFFFFFFFF, np.uint32)
+    dists = np.full((len(queries), max_k), 0, np.int32)
+    comps = np.zeros(len(queries), np.int32)
+    exps = np.zeros(len(queries), np.int32)
+    for L in np.unique(ls):
+        for k in np.unique(ks):
+            sel = np.nonzero((ls == L) & (ks == k))[0]
+            if not len(sel):
+                continue
+            for q in sel:  # query index matters (exclusion quirk): one call per query
+                o = oracle.flat_search(base, graph.degrees, graph.edges, queries[q:q + 1], int(k),
+                                       int(L), query_id_base=int(q), **kw)
+                ids[q, :k], dists[q, :k], comps[q], exps[q] = o[0][0], o[1][0], o[2][0], o[3][0]
+    return ids, dists, comps, exps
+
+
+@pytest.mark.parametrize("graph_name", ["vamana", "hcnng"])
+def test_batch_mixed_beams_match_oracle(pgb, oracle, golden, gpu, graph_name):
+    import torch
+    base, queries = golden.vectors_for(graph_name)
+    graph = golden.graphs[graph_name]
+    rng = np.random.default_rng(11)
+    nq = len(queries)
+    ls = rng.choice([10, 16, 25, 40, 63, 100, 160], size=nq).astype(np.uint32)
+    ks = rng.choice([10, 50], size=nq).astype(np.uint32)
+    max_k = 50
+    index = pgb.Index.flat(base, graph)
+    b = pgb.Batch(index, nq, max_beam=int(ls.max()), max_k=max_k)
+    b.plan(ls, ks)
+    q = torch.from_numpy(queries.view(np.uint8)).cuda()
+    ids, dists, stats = b.outputs(q.device)
+    b.search(q, ids, dists, stats)
+    torch.cuda.synchronize()
+    oid, od, oc, oe = oracle_rows(oracle, base, graph, queries, ls, ks, max_k)
+    got_i = ids.cpu().numpy().view(np.uint32)
+    got_d = dists.cpu().numpy()
+    st = stats.cpu().numpy()
+    for qi in range(nq):
+        k = ks[qi]
+        assert_same(f"q{qi} ids", got_i[qi, :k], oid[qi, :k])
+        assert_same(f"q{qi} dists", got_d[qi, :k], od[qi, :k])
+    assert_same("comps", st[:, 0], oc)
+    assert_same("expansions", st[:, 1], oe)
+    # every tuned configuration and the captured graph give the same answer
+    cfg = b.tune(q, ids, dists, stats)
+    assert cfg["tuned_ms"] > 0
+    b.capture(q, ids, dists, stats)
+    ids.fill_(0)
+    b.replay()
+    torch.cuda.synchronize()
+    for qi in range(nq):
+        k = ks[qi]
+        assert_same(f"replay q{qi}", ids.cpu().numpy().view(np.uint32)[qi, :k], oid[qi, :k])
+    b.close()
+    index.close()
+
+
+@pytest.mark.parametrize("placement", [(1, 1), (1, 2), (2, 1), (2, 2)])
+def test_batch_placements_identical(pgb, golden, gpu, placement):
+    import torch
+    base, queries = golden.vectors_for("vamana")
+    index = pgb.Index.flat(base, golden.graphs["vamana"])
+    nq = len(queries)
+    s = pgb.Searcher(index, nq, pgb.QueryParams(k=10, beam_size=80))
+    want_i, want_d, _ = s.search(queries)
+    b = pgb.Batch(index, nq, max_beam=80, max_k=10, filter_placement=placement[0],
+                  visited_placement=placement[1], warps_per_block=2)
+    b.plan(np.full(nq, 80), np.full(nq, 10))
+    q = torch.from_numpy(queries.view(np.uint8)).cuda()
+    ids, dists, stats = b.outputs(q.device)
+    b.search(q, ids, dists, stats)
+    torch.cuda.synchronize()
+    cfg = b.config()
+    assert cfg["filter_in_shared"] == (placement[0] == 1)
+    assert cfg["visited_in_shared"] == (placement[1] == 1)
+    assert_same("ids", ids.cpu().numpy().view(np.uint32), want_i)
+    assert_same("dists", dists.cpu().numpy(), want_d)
