@@ -163,7 +163,7 @@ typedef struct pgb_batch_options {
     uint32_t degree_limit;      /* 0: graph max degree                                  */
     uint32_t exclude_query_id;
     uint32_t query_id_base;
-    uint32_t warps_per_block;   /* 0: default / tuned                                   */
+    uint32_t warps_per_block;   /* 1, 2 or 4; 0: default (4) / tuned                    */
     uint32_t filter_placement;  /* 0 auto, 1 shared memory, 2 global memory             */
     uint32_t visited_placement; /* 0 auto, 1 shared memory, 2 global memory             */
 } pgb_batch_options;
@@ -182,6 +182,10 @@ pgb_status pgb_batch_plan(pgb_batch* b, const uint32_t* beam_sizes, const uint32
 pgb_status pgb_batch_search(pgb_batch* b, const void* queries, uint32_t query_stride,
                             uint32_t* ids, int32_t* dists, pgb_query_stats* stats,
                             void* stream);
+/* Same launch from and to HOST memory, synchronous: upload of the planned queries,
+ * one launch, download of ids / dists / stats (stats may be NULL); row stride max_k. */
+pgb_status pgb_batch_search_host(pgb_batch* b, const void* queries, uint32_t query_stride,
+                                 uint32_t* ids, int32_t* dists, pgb_query_stats* stats);
 /* Autotuner: times the candidate launch shapes and table placements on the planned
  * queries (outputs are overwritten) and keeps the fastest. Synchronous. */
 pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t query_stride,

@@ -115,6 +115,7 @@ _sig("pgb_batch_create", C.c_int, vp, C.POINTER(BatchOptions), C.POINTER(vp))
 _sig("pgb_batch_plan", C.c_int, vp, vp, vp, u32)
 _sig("pgb_batch_search", C.c_int, vp, vp, u32, vp, vp, vp, vp)
 _sig("pgb_batch_tune", C.c_int, vp, vp, u32, vp, vp, vp)
+_sig("pgb_batch_search_host", C.c_int, vp, vp, u32, vp, vp, vp)
 _sig("pgb_batch_get_config", C.c_int, vp, C.POINTER(BatchConfig))
 _sig("pgb_batch_capture", C.c_int, vp, vp, u32, vp, vp, vp)
 _sig("pgb_batch_replay", C.c_int, vp, vp)

@@ -32,6 +32,12 @@ struct pgb_batch {
     uint32_t max_ls_planned = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    // host-memory path staging
+    uint8_t* q_dev = nullptr;
+    uint32_t* ids_dev = nullptr;
+    int32_t* dists_dev = nullptr;
+    pgb_query_stats* stats_dev = nullptr;
+    cudaStream_t stream = nullptr;
 };
 
 namespace pgb {
@@ -105,6 +111,7 @@ pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_
     A.limit = b->opt.limit <= 0 ? (int64_t)ix->n : b->opt.limit;
     A.excl = b->opt.exclude_query_id ? 1u : 0u;
     A.qbase = b->opt.query_id_base;
+    A.norm_in_row = ix->norm_in_row ? 1u : 0u;
     A.ls_arr = b->d_ls;
     A.k_arr = b->d_k;
     A.order = b->d_order;
@@ -142,7 +149,7 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
     if (opt->max_queries == 0 || opt->max_beam == 0 || opt->max_beam > PGB_MAX_BEAM ||
         opt->max_k == 0 || opt->max_k > PGB_MAX_K || !(opt->cut > 0))
         return fail(PGB_ERR_BAD_ARG, "bad max_queries / max_beam / max_k / cut");
-    if (opt->warps_per_block > 8 || opt->filter_placement > 2 || opt->visited_placement > 2)
+    if (opt->warps_per_block > 4 || opt->filter_placement > 2 || opt->visited_placement > 2)
         return fail(PGB_ERR_BAD_ARG, "bad launch shape or placement option");
     DeviceGuard guard(ix->device);
     if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
@@ -157,7 +164,12 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
         (s = cuda_status(cudaMalloc(&b->d_ls, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_k, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_order, 4 * nq), "batch arrays")) != PGB_OK ||
-        (s = cuda_status(cudaMalloc(&b->d_queue, 4), "batch counter")) != PGB_OK) {
+        (s = cuda_status(cudaMalloc(&b->d_queue, 4), "batch counter")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->q_dev, nq * ix->dim), "query staging")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->ids_dev, 4 * nq * opt->max_k), "ids staging")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->dists_dev, 4 * nq * opt->max_k), "dists staging")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&b->stats_dev, sizeof(pgb_query_stats) * nq), "stats staging")) != PGB_OK ||
+        (s = cuda_status(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking), "stream")) != PGB_OK) {
         pgb_batch_destroy(b);
         return s;
     }
@@ -203,6 +215,35 @@ pgb_status pgb_batch_search(pgb_batch* b, const void* queries, uint32_t qstride,
     return enqueue(b, b->plan, queries, qstride, ids, dists, stats, (cudaStream_t)stream);
 }
 
+pgb_status pgb_batch_search_host(pgb_batch* b, const void* queries, uint32_t qstride,
+                                 uint32_t* ids, int32_t* dists, pgb_query_stats* stats) {
+    pgb_status s = check_call(b, queries, qstride, ids, dists);
+    if (s != PGB_OK) return s;
+    DeviceGuard guard(b->index->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    const pgb_index* ix = b->index;
+    const size_t nq = b->nq, row = 4ull * b->opt.max_k;
+    cudaStream_t st = b->stream;
+    cudaError_t ce = (qstride == ix->dim)
+                         ? cudaMemcpyAsync(b->q_dev, queries, nq * ix->dim, cudaMemcpyHostToDevice, st)
+                         : cudaMemcpy2DAsync(b->q_dev, ix->dim, queries, qstride, ix->dim, nq,
+                                             cudaMemcpyHostToDevice, st);
+    if ((s = cuda_status(ce, "query upload")) != PGB_OK) return s;
+    if ((s = enqueue(b, b->plan, b->q_dev, ix->dim, b->ids_dev, b->dists_dev,
+                     stats ? b->stats_dev : nullptr, st)) != PGB_OK)
+        return s;
+    if ((s = cuda_status(cudaMemcpyAsync(ids, b->ids_dev, nq * row, cudaMemcpyDeviceToHost, st),
+                         "ids download")) != PGB_OK ||
+        (s = cuda_status(cudaMemcpyAsync(dists, b->dists_dev, nq * row, cudaMemcpyDeviceToHost, st),
+                         "dists download")) != PGB_OK)
+        return s;
+    if (stats && (s = cuda_status(cudaMemcpyAsync(stats, b->stats_dev, sizeof(pgb_query_stats) * nq,
+                                                  cudaMemcpyDeviceToHost, st),
+                                  "stats download")) != PGB_OK)
+        return s;
+    return cuda_status(cudaStreamSynchronize(st), "batch search");
+}
+
 pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
                           int32_t* dists, pgb_query_stats* stats) {
     pgb_status s = check_call(b, queries, qstride, ids, dists);
@@ -215,7 +256,7 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const int wpbs[] = {2, 4, 8};
+    const int wpbs[] = {1, 2, 4};
     const int fpls[] = {1, 2};
     const int vpls[] = {1, 2};
     float best = 1e30f;
@@ -286,6 +327,7 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
         if (ls != PGB_OK) {
             if (g) cudaGraphDestroy(g);
             cudaStreamDestroy(st);
+            cudaGetLastError();  // the invalidated capture must not leak into later calls
             return ls;
         }
         if (e == cudaSuccess) {
@@ -296,7 +338,7 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
     cudaStreamDestroy(st);
     if (e != cudaSuccess) {
         drop_graph(b);
-        return cuda_status(e, "graph capture");
+        return cuda_status(e, "graph capture");  // cuda_status clears the error state
     }
     return PGB_OK;
 }
@@ -317,6 +359,11 @@ pgb_status pgb_batch_destroy(pgb_batch* b) {
     cudaFree(b->d_k);
     cudaFree(b->d_order);
     cudaFree(b->d_queue);
+    cudaFree(b->q_dev);
+    cudaFree(b->ids_dev);
+    cudaFree(b->dists_dev);
+    cudaFree(b->stats_dev);
+    if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return PGB_OK;
 }

@@ -80,6 +80,26 @@ __device__ __forceinline__ int32_t partial_l2(const int4 p, const int4 q) {
     return pp - 2 * pq;
 }
 
+// dot(p, q) over 16 bytes
+template <bool Signed>
+__device__ __forceinline__ int32_t partial_dot(const int4 p, const int4 q) {
+    if (Signed) {
+        int32_t s = __dp4a(p.x, q.x, 0);
+        s = __dp4a(p.y, q.y, s);
+        s = __dp4a(p.z, q.z, s);
+        return __dp4a(p.w, q.w, s);
+    } else {
+        uint32_t s = __dp4a((uint32_t)p.x, (uint32_t)q.x, 0u);
+        s = __dp4a((uint32_t)p.y, (uint32_t)q.y, s);
+        s = __dp4a((uint32_t)p.z, (uint32_t)q.z, s);
+        return (int32_t)__dp4a((uint32_t)p.w, (uint32_t)q.w, s);
+    }
+}
+
+// Rows of at most 124 meaningful bytes carry their squared norm (int32) in bytes
+// 124..127; the query row has zeros there, so it drops out of every dot product.
+constexpr uint32_t kNormInRowMaxDim = 124;
+
 template <bool Signed>
 __device__ __forceinline__ int32_t partial_sq(const int4 q) {
     if (Signed) {
@@ -98,6 +118,11 @@ __device__ __forceinline__ int32_t partial_sq(const int4 q) {
 // read-only 16-byte load through the non-coherent path
 __device__ __forceinline__ int4 ldg16(const void* p) {
     return __ldg(reinterpret_cast<const int4*>(p));
+}
+
+// Hint: bring the line of one 128-byte row into L2 (no register or completion cost).
+__device__ __forceinline__ void prefetch_row_l2(const void* p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
 // Loads a query of `dim` bytes (any alignment) into a zero-padded 128-byte row in

@@ -7,6 +7,7 @@
 #include <string>
 #include <vector>
 
+#include "device_common.cuh"
 #include "errors.h"
 #include "formats.h"
 #include "index.h"
@@ -32,6 +33,22 @@ __global__ void pad_rows_kernel(const uint8_t* __restrict__ packed, uint32_t n, 
     int4 v;
     memcpy(&v, b, 16);
     reinterpret_cast<int4*>(rows + r * 128)[w] = v;
+}
+
+// squared norm of each row into bytes 124..127 (rows of at most 124 meaningful bytes)
+template <bool Signed>
+__global__ void norm_rows_kernel(uint8_t* __restrict__ rows, uint32_t n) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int4* row = reinterpret_cast<int4*>(rows + r * 128);
+    int32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+        int4 v = row[w];
+        if (w == 7) v.w = 0;
+        s += partial_sq<Signed>(v);
+    }
+    reinterpret_cast<int32_t*>(rows + r * 128)[31] = s;
 }
 
 // CSR rows -> fixed-stride rows padded with 0xFFFFFFFF, one thread per slot
@@ -73,9 +90,10 @@ pgb_status upload(void* dst, const void* src, size_t bytes, const char* what) {
     return e == cudaSuccess ? PGB_OK : cuda_fail(e, what);
 }
 
-// packed host vectors -> padded device rows (optionally gathered by node)
-pgb_status make_rows(const void* vectors, uint32_t n_src, uint32_t dim, const uint32_t* gather,
-                     uint32_t n_out, uint8_t** rows) {
+// packed host vectors -> padded device rows (optionally gathered by node); rows of at
+// most 124 bytes get their squared norm in bytes 124..127
+pgb_status make_rows(const void* vectors, uint32_t n_src, uint32_t dim, bool is_signed,
+                     const uint32_t* gather, uint32_t n_out, uint8_t** rows) {
     DevBuf packed, g;
     pgb_status s = dev_alloc(&packed.p, (size_t)n_src * dim, "vectors");
     if (s != PGB_OK) return s;
@@ -88,6 +106,11 @@ pgb_status make_rows(const void* vectors, uint32_t n_src, uint32_t dim, const ui
     const uint64_t threads = 8ull * n_out;
     pad_rows_kernel<<<(unsigned)((threads + 255) / 256), 256>>>(
         (const uint8_t*)packed.p, n_out, dim, (const uint32_t*)g.p, *rows);
+    if (dim <= kNormInRowMaxDim) {
+        const unsigned nb = (unsigned)((n_out + 255ull) / 256);
+        if (is_signed) norm_rows_kernel<true><<<nb, 256>>>(*rows, n_out);
+        else norm_rows_kernel<false><<<nb, 256>>>(*rows, n_out);
+    }
     cudaError_t e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = cudaGetLastError();
     return e == cudaSuccess ? PGB_OK : cuda_fail(e, "pad rows");
@@ -197,7 +220,8 @@ pgb_status pgb_index_create_flat(int device, const void* vectors, uint32_t n, ui
     ix->G = std::max<uint32_t>(G, 1);
     ix->gs = round32(ix->G);
     std::vector<uint32_t> sizes(degrees, degrees + n);
-    if ((s = make_rows(vectors, n, dim, nullptr, n, &ix->rows)) != PGB_OK ||
+    ix->norm_in_row = dim <= kNormInRowMaxDim;
+    if ((s = make_rows(vectors, n, dim, elem == PGB_INT8, nullptr, n, &ix->rows)) != PGB_OK ||
         (s = make_matrix(sizes, edges, total, ix->gs, &ix->adj)) != PGB_OK) {
         free_index(ix);
         return s;
@@ -303,14 +327,16 @@ pgb_status pgb_index_create_hnsw(int device, const void* vectors, uint32_t n_poi
     }
     bool identity = n_nodes == n_points;
     for (uint32_t i = 0; i < n_nodes && identity; i++) identity = node_point[i] == i;
-    if ((s = make_rows(vectors, n_points, dim, nullptr, n_points, &ix->rows)) != PGB_OK) {
+    ix->norm_in_row = dim <= kNormInRowMaxDim;
+    if ((s = make_rows(vectors, n_points, dim, elem == PGB_INT8, nullptr, n_points, &ix->rows)) !=
+        PGB_OK) {
         free_index(ix);
         return s;
     }
     if (identity) {
         ix->node_rows = ix->rows;
-    } else if ((s = make_rows(vectors, n_points, dim, node_point, n_nodes, &ix->node_rows)) !=
-               PGB_OK) {
+    } else if ((s = make_rows(vectors, n_points, dim, elem == PGB_INT8, node_point, n_nodes,
+                              &ix->node_rows)) != PGB_OK) {
         free_index(ix);
         return s;
     }

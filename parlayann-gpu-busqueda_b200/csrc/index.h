@@ -1,8 +1,9 @@
 // index.h -- device-resident index: 128-byte vector rows + fixed-stride adjacency.
 //
 // HBM layout
-//   rows       : n x 128 B, vector bytes then zeros (int8 d=100 or uint8 d=128); the
-//                squared norm is recomputed from the row, so no norm array exists
+//   rows       : n x 128 B, vector bytes then zeros (int8 d=100 or uint8 d=128); when
+//                the vector has at most 124 bytes, its int32 squared norm fills bytes
+//                124..127, so no separate norm array is gathered (d=128: recomputed)
 //   adj        : n x gs u32, gs = degree rounded up to 32 (128-byte aligned rows),
 //                padded with 0xFFFFFFFF (reference GrafoGPU, cuda/datos_gpu.h:19-28)
 //   HNSW       : level-0 matrix n x g0s; upper levels one block of gas ids per
@@ -21,6 +22,7 @@ struct pgb_index {
     uint32_t n = 0, dim = 0;
     pgb_elem elem = PGB_INT8;
     bool is_hnsw = false;
+    bool norm_in_row = false;  // rows hold their squared norm in bytes 124..127
     uint8_t* rows = nullptr;  // point order
     // flat graph
     uint32_t* adj = nullptr;

@@ -15,7 +15,7 @@
 namespace pgb {
 
 template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(256) flat_plain_kernel(FlatArgs A) {
+__global__ void __launch_bounds__(128, 9) flat_plain_kernel(FlatArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(256) flat_plain_kernel(FlatArgs A) {
 }
 
 template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(256) flat_batched_kernel(FlatArgs A) {
+__global__ void __launch_bounds__(128, 9) flat_batched_kernel(FlatArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -105,14 +105,20 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
         return fail(PGB_ERR_CUDA, "cudaGetDeviceProperties failed");
     const size_t smem_cap = prop.sharedMemPerBlockOptin;
-    int wpb = rq.warps_per_block > 0 ? rq.warps_per_block : 4;
+    // at most 4 warps per block: the kernels are built for 128 threads, 9 blocks per SM
+    int wpb = rq.warps_per_block > 0 ? std::min(rq.warps_per_block, 4) : 4;
     while (wpb > 1 && (size_t)wpb * P.L.bytes > smem_cap) wpb >>= 1;
     if ((size_t)wpb * P.L.bytes > smem_cap)
         return fail(PGB_ERR_BAD_ARG, "beam too wide for shared memory with this placement");
     P.warps_per_block = wpb;
     P.smem_bytes = (size_t)wpb * P.L.bytes;
+    // the attribute belongs to the kernel, shared by every plan of it: set the device
+    // maximum so that no later plan can shrink it under an earlier one
     cudaError_t e = cudaFuncSetAttribute(P.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)P.smem_bytes);
+                                         (int)smem_cap);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(P.kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess)
         return fail(PGB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
     int bps = 0;

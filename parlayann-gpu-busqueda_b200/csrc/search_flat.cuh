@@ -92,6 +92,7 @@ struct FlatArgs {
     double cut;
     int64_t limit;         // resolved: > 0
     uint32_t excl, qbase;
+    uint32_t norm_in_row;           // rows carry their squared norm in bytes 124..127
     uint32_t Ls, k;                 // uniform values (plain kernel)
     const uint32_t* ls_arr;         // per-query Ls (batched), indexed by query
     const uint32_t* k_arr;          // per-query k (batched)
@@ -212,11 +213,22 @@ __device__ __forceinline__ void sort_keys_e(uint64_t* keys, int nc, int lane) {
     __syncwarp();
 }
 
-// sorts keys[0..nc) ascending; nc <= 32 * CH
+// sorts keys[0..nc) ascending; nc <= 32 * CH. Few keys: each lane counts the keys below
+// its own and scatters it to that rank (equal keys are identical, so their order is moot).
 template <int CH>
 __device__ __forceinline__ void sort_keys(uint64_t* keys, int nc, int lane) {
     if (nc <= 1) return;
-    if (nc <= 32) {
+    if (nc <= 20) {
+        const uint64_t mine = lane < nc ? keys[lane] : 0;
+        int rank = 0;
+        for (int j = 0; j < nc; j++) {
+            const uint64_t o = keys[j];
+            rank += (o < mine || (o == mine && j < lane)) ? 1 : 0;
+        }
+        __syncwarp();
+        if (lane < nc) keys[rank] = mine;
+        __syncwarp();
+    } else if (nc <= 32) {
         sort_keys_e<1>(keys, nc, lane);
     } else if (CH >= 2 && nc <= 64) {
         sort_keys_e<(CH >= 2 ? 2 : 1)>(keys, nc, lane);
@@ -228,13 +240,15 @@ __device__ __forceinline__ void sort_keys(uint64_t* keys, int nc, int lane) {
 }
 
 // ---- distances of pending rows: 8 lanes per 128-byte row, 16 rows in flight ---------
+// norm_in_row: the row's squared norm sits in bytes 124..127 (lane 7's last word)
 template <bool Signed>
 __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
                                               const uint32_t* ids, int32_t* out, int np,
                                               const int4 qv, const int32_t qq, uint32_t dim,
-                                              int lane) {
+                                              bool norm_in_row, int lane) {
     const int grp = lane >> 3, sub = lane & 7;
-    const bool need = (uint32_t)(sub * 16) < dim;  // bytes past dim are zero in every row
+    // bytes past dim are zero in every row; lane 7 also loads when it holds the norm
+    const bool need = (uint32_t)(sub * 16) < dim || (norm_in_row && sub == 7);
     for (int base = 0; base < np; base += 16) {
         int4 v[4];
 #pragma unroll
@@ -244,8 +258,14 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
             if (i < np && need) v[r] = ldg16(rows + (size_t)ids[i] * kRowBytes + sub * 16);
         }
         int32_t t[4];
+        if (norm_in_row) {
 #pragma unroll
-        for (int r = 0; r < 4; r++) t[r] = partial_l2<Signed>(v[r], qv);
+            for (int r = 0; r < 4; r++)
+                t[r] = (sub == 7 ? v[r].w : 0) - 2 * partial_dot<Signed>(v[r], qv);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 4; r++) t[r] = partial_l2<Signed>(v[r], qv);
+        }
 #pragma unroll
         for (int off = 4; off > 0; off >>= 1)
 #pragma unroll
@@ -290,9 +310,14 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
 
     // query row (zero padded) and ||q||^2
     load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
-    // clear this query's tables
-    for (uint32_t i = lane; i <= fmask; i += 32) filter[i] = kEmptyId;
-    for (uint32_t i = lane; i < vcap; i += 32) vtab[i] = kEmptyId;
+    // clear this query's tables (both sizes are multiples of 128 words, 16-byte aligned)
+    {
+        const uint4 e4 = make_uint4(kEmptyId, kEmptyId, kEmptyId, kEmptyId);
+        uint4* f4 = reinterpret_cast<uint4*>(filter);
+        for (uint32_t i = lane; i < (fmask + 1u) / 4u; i += 32) f4[i] = e4;
+        uint4* v4 = reinterpret_cast<uint4*>(vtab);
+        for (uint32_t i = lane; i < vcap / 4u; i += 32) v4[i] = e4;
+    }
     __syncwarp();
     const int4 qv = reinterpret_cast<const int4*>(qwords)[lane & 7];
     int32_t qq = partial_sq<Signed>(qv);
@@ -302,7 +327,8 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     // start point: F = {(d(q, start), start)}, one distance
     if (lane == 0) pend[0] = A.start;
     __syncwarp();
-    row_distances<Signed>(A.rows, pend, pdist, 1, qv, qq, A.dim, lane);
+    const bool nir = A.norm_in_row != 0;
+    row_distances<Signed>(A.rows, pend, pdist, 1, qv, qq, A.dim, nir, lane);
     if (lane == 0) {
         fkey[0] = pack_key(pdist[0], A.start);
         fvis[0] = 0;
@@ -313,17 +339,26 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     int nvis = 0;
     int comps = 1;
     const int deg_lim = (int)A.deg_lim;
+    // row of the predicted next expansion, loaded while the current one is merged
+    uint32_t pred = kEmptyId;
+    uint32_t apred[CH];
+    int u2 = -1;  // second unvisited frontier entry when known
 
     while (u >= 0 && (int64_t)nvis < limit) {
         const uint64_t cur_key = fkey[u];
         const uint32_t cur = key_id(cur_key);
-        // whole neighbour row, requested before it is needed
+        // whole neighbour row: the predicted one, or requested now
         uint32_t a[CH];
-        const uint32_t* row = A.adj + (size_t)cur * A.gs;
+        if (cur == pred) {
 #pragma unroll
-        for (int t = 0; t < CH; t++) {
-            const int j = t * 32 + lane;
-            a[t] = (j < deg_lim) ? __ldg(row + j) : kEmptyId;
+            for (int t = 0; t < CH; t++) a[t] = apred[t];
+        } else {
+            const uint32_t* row = A.adj + (size_t)cur * A.gs;
+#pragma unroll
+            for (int t = 0; t < CH; t++) {
+                const int j = t * 32 + lane;
+                a[t] = (j < deg_lim) ? __ldg(row + j) : kEmptyId;
+            }
         }
         if (lane == 0) fvis[u] = 1;
         visited_insert(vtab, vmask, cur, lane);
@@ -408,7 +443,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         comps += np;
 
         // ---- distances ------------------------------------------------------------
-        row_distances<Signed>(A.rows, pend, pdist, np, qv, qq, A.dim, lane);
+        row_distances<Signed>(A.rows, pend, pdist, np, qv, qq, A.dim, nir, lane);
 
         // ---- candidates under the cutoff, in arrival order ------------------------
         int nc = 0;
@@ -420,12 +455,16 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
             nc += __popc(m);
         }
         __syncwarp();
+        // the next expansion is the smaller of the second unvisited entry and the best
+        // unvisited candidate that enters the frontier (unless the cut drops it); its row
+        // is requested as soon as that is known, before the frontier is shifted
+        uint64_t best = (u2 >= 0 && u2 < fsize) ? fkey[u2] : kEmptyKey;
 
         int unew = u, minpos = INT_MAX;
+        int ne = 0;
         if (nc > 0) {
             sort_keys<CH>(ckey, nc, lane);
             // ---- multiset set_union: copy `rep` of a key enters iff rep >= copies in F
-            int ne = 0;
             for (int base = 0; base < nc; base += 32) {
                 const int i = base + lane;
                 bool enter = false;
@@ -447,6 +486,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 // new copies follow the frontier copies of an equal key
                 const int pos = hi + ne + __popc(m & lt);
                 const bool keep = enter && pos < (int)Ls;
+                if (keep && !vis) best = key < best ? key : best;
                 const uint32_t mk = __ballot_sync(kFull, keep);
                 if (keep) {
                     const int jk = ne + __popc(mk & lt);
@@ -458,6 +498,22 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 if (mk != m) break;  // later keys land at or past Ls
             }
             __syncwarp();
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const uint64_t o = __shfl_xor_sync(kFull, best, off);
+                best = o < best ? o : best;
+            }
+        }
+        pred = (best != kEmptyKey) ? key_id(best) : kEmptyId;
+        if (pred != kEmptyId) {
+            const uint32_t* prow = A.adj + (size_t)pred * A.gs;
+#pragma unroll
+            for (int t = 0; t < CH; t++) {
+                const int j = t * 32 + lane;
+                apred[t] = (j < deg_lim) ? __ldg(prow + j) : kEmptyId;
+            }
+        }
+        {
             if (ne > 0) {
                 // the expanded entry's new position, then shift the frontier tail
                 unew = u + lower_bound_key(ekey, ne, cur_key);
@@ -516,14 +572,24 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         for (int off = 16; off > 0; off >>= 1) minpos = min(minpos, __shfl_xor_sync(kFull, minpos, off));
         const int from = min(unew, minpos);
         u = -1;
+        u2 = -1;
         for (int base = from; base < fsize; base += 32) {
             const int i = base + lane;
             const bool un = i < fsize && !fvis[i];
             const uint32_t m = __ballot_sync(kFull, un);
             if (m) {
                 u = base + __ffs(m) - 1;
+                const uint32_t rest = m & (m - 1);
+                u2 = rest ? base + __ffs(rest) - 1 : -1;
                 break;
             }
+        }
+        // the prediction held: pull the vector rows of its neighbours into L2 now, ahead
+        // of the next distance phase (rows the filter will drop are fetched too)
+        if (u >= 0 && key_id(fkey[u]) == pred) {
+#pragma unroll
+            for (int t = 0; t < CH; t++)
+                if (apred[t] != kEmptyId) prefetch_row_l2(A.rows + (size_t)apred[t] * kRowBytes);
         }
         __syncwarp();
     }

@@ -82,7 +82,7 @@ struct HnswArgs {
     const uint32_t* upper_start;
     const uint32_t* node_point;
     uint32_t entries[PGB_MAX_HNSW_ENTRIES];
-    uint32_t n_entries, top, dim;
+    uint32_t n_entries, top, dim, norm_in_row;
     const uint8_t* queries;
     uint32_t nq, qstride;
     uint32_t Ls, k;
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
             // ---- entry points: distances, then the sequential inserts on lane 0 ----
             for (int e = lane; e < neps; e += 32) pend[e] = eps[e];
             __syncwarp();
-            row_distances<Signed>(A.rows, pend, pd, neps, qv, qq, A.dim, lane);
+            row_distances<Signed>(A.rows, pend, pd, neps, qv, qq, A.dim, A.norm_in_row != 0, lane);
             int nC = 0;
             nW = 0;
             if (lane == 0) {
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
                     }
                 }
                 comps += np;
-                row_distances<Signed>(A.rows, pend, pd, np, qv, qq, A.dim, lane);
+                row_distances<Signed>(A.rows, pend, pd, np, qv, qq, A.dim, A.norm_in_row != 0, lane);
 
                 // ---- eligibility: first copy in this expansion and not in is_inw ------
                 for (int j = lane; j < np; j += 32) {
@@ -527,8 +527,9 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
         return fail(PGB_ERR_BAD_ARG, "beam too wide for shared memory");
     H.warps_per_block = wpb;
     H.smem_bytes = (size_t)wpb * L.bytes;
+    // per-kernel attribute shared by all searchers: the device maximum, never shrunk
     if ((s = hnsw_cuda(cudaFuncSetAttribute(H.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)H.smem_bytes),
+                                            (int)prop.sharedMemPerBlockOptin),
                        "cudaFuncSetAttribute")) != PGB_OK)
         return s;
     int bps = 0;
@@ -569,6 +570,7 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     A.n_entries = ix->n_entries;
     A.top = ix->top_level;
     A.dim = ix->dim;
+    A.norm_in_row = ix->norm_in_row ? 1u : 0u;
     A.queries = (const uint8_t*)queries;
     A.nq = nq;
     A.qstride = qstride;

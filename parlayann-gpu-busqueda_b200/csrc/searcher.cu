@@ -119,6 +119,7 @@ pgb_status pgb_searcher_search(pgb_searcher* S, const void* queries, uint32_t nq
     A.limit = (p.limit <= 0) ? (int64_t)ix->n : p.limit;
     A.excl = p.exclude_query_id ? 1u : 0u;
     A.qbase = p.query_id_base;
+    A.norm_in_row = ix->norm_in_row ? 1u : 0u;
     A.Ls = p.beam_size;
     A.k = p.k;
     A.out_stride = p.k;
@@ -144,11 +145,13 @@ pgb_status pgb_searcher_search_host(pgb_searcher* S, const void* queries, uint32
     const size_t k = S->params.k;
     cudaStream_t st = S->stream;
     pgb_status s;
-    // queries packed to dim bytes on the way in
-    if ((s = cuda_status(cudaMemcpy2DAsync(S->q_dev, ix->dim, queries, query_stride, ix->dim, nq,
-                                           cudaMemcpyHostToDevice, st),
-                         "query upload")) != PGB_OK)
-        return s;
+    // queries packed to dim bytes on the way in (one linear copy when already packed)
+    cudaError_t ce =
+        (query_stride == ix->dim)
+            ? cudaMemcpyAsync(S->q_dev, queries, (size_t)nq * ix->dim, cudaMemcpyHostToDevice, st)
+            : cudaMemcpy2DAsync(S->q_dev, ix->dim, queries, query_stride, ix->dim, nq,
+                                cudaMemcpyHostToDevice, st);
+    if ((s = cuda_status(ce, "query upload")) != PGB_OK) return s;
     if ((s = pgb_searcher_search(S, S->q_dev, nq, ix->dim, S->ids_dev, S->dists_dev,
                                  stats ? S->stats_dev : nullptr, st)) != PGB_OK)
         return s;

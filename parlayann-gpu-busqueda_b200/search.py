@@ -258,6 +258,19 @@ class Batch:
         q, st, i, d, s = self._args(queries, ids, dists, stats)
         N.check(N.lib.pgb_batch_search(self._h, q, st, i, d, s, C.c_void_p(stream)))
 
+    def search_host(self, queries: np.ndarray, ids=None, dists=None, stats=None):
+        """Host queries (planned count) -> host ids/dists/stats, synchronous. Pass pinned
+        numpy/torch buffers to avoid staging copies in the driver."""
+        q = queries if not isinstance(queries, np.ndarray) else np.ascontiguousarray(queries)
+        if ids is None:
+            ids = np.empty((self.nq, self.max_k), dtype=np.uint32)
+            dists = np.empty((self.nq, self.max_k), dtype=np.int32)
+            stats = np.empty((self.nq, 4), dtype=np.int32)
+        stride = q.stride(0) if hasattr(q, "stride") else q.shape[1]
+        N.check(N.lib.pgb_batch_search_host(self._h, _ptr(q), stride, _ptr(ids), _ptr(dists),
+                                            _ptr(stats)))
+        return ids, dists, stats
+
     def tune(self, queries, ids, dists, stats=None):
         q, st, i, d, s = self._args(queries, ids, dists, stats)
         N.check(N.lib.pgb_batch_tune(self._h, q, st, i, d, s))

@@ -86,3 +86,17 @@ def test_batch_placements_identical(pgb, golden, gpu, placement):
     assert cfg["visited_in_shared"] == (placement[1] == 1)
     assert_same("ids", ids.cpu().numpy().view(np.uint32), want_i)
     assert_same("dists", dists.cpu().numpy(), want_d)
+
+
+def test_batch_host_path_matches_device(pgb, oracle, golden, gpu):
+    base, queries = golden.vectors_for("nnd")
+    graph = golden.graphs["nnd"]
+    index = pgb.Index.flat(base, graph)
+    nq = len(queries)
+    b = pgb.Batch(index, nq, max_beam=40, max_k=10)
+    b.plan(np.full(nq, 40), np.full(nq, 10))
+    ids, dists, stats = b.search_host(queries)
+    oid, od, oc, oe, of = oracle.flat_search(base, graph.degrees, graph.edges, queries, 10, 40)
+    assert_same("ids", ids, oid)
+    assert_same("dists", dists, od)
+    assert_same("comps", stats[:, 0], oc)

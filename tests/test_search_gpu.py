@@ -40,3 +40,41 @@ def test_flat_matches_oracle(pgb, oracle, golden, gpu, graph_name, cfg):
     assert_same("comps", stats[:, 0], oc)
     assert_same("expansions", stats[:, 1], oe)
     assert_same("flags", stats[:, 2], of)
+
+
+def test_searchers_with_different_beams_coexist(pgb, oracle, golden, gpu):
+    """Several live searchers of one kernel variant keep working after each other's
+    creation (their launch shapes differ; none may shrink another's limits)."""
+    base, queries = golden.vectors_for("vamana")
+    g = golden.graphs["vamana"]
+    index = pgb.Index.flat(base, g)
+    wide = pgb.Searcher(index, len(queries), pgb.QueryParams(k=10, beam_size=120))
+    narrow = pgb.Searcher(index, len(queries), pgb.QueryParams(k=10, beam_size=12))
+    for s, Ls in ((wide, 120), (narrow, 12), (wide, 120)):
+        ids, dists, _ = s.search(queries)
+        oid, od, *_ = oracle.flat_search(base, g.degrees, g.edges, queries, 10, Ls)
+        assert_same(f"ids Ls={Ls}", ids, oid)
+        assert_same(f"dists Ls={Ls}", dists, od)
+
+
+def test_query_id_base_and_exclusion_off(pgb, oracle, golden, gpu):
+    """The exclusion quirk follows query_id_base; with exclusion off every id is eligible."""
+    base, queries = golden.vectors_for("vamana")
+    g = golden.graphs["vamana"]
+    for excl, qb in ((True, 37), (False, 0)):
+        (ids, dists, st), (oid, od, oc, oe, of) = run_both(
+            pgb, oracle, base, queries, g, 30, 0, 10, 1.35, exclude_query_id=excl,
+            query_id_base=qb)
+        assert_same(f"ids excl={excl}", ids, oid)
+        assert_same(f"comps excl={excl}", st[:, 0], oc)
+
+
+@pytest.mark.parametrize("deg_lim", [1, 7, 20, 31])
+def test_degree_limit(pgb, oracle, golden, gpu, deg_lim):
+    base, queries = golden.vectors_for("hcnng")
+    g = golden.graphs["hcnng"]
+    (ids, dists, st), (oid, od, oc, oe, of) = run_both(
+        pgb, oracle, base, queries, g, 40, 0, 10, 1.35, degree_limit=deg_lim)
+    assert_same("ids", ids, oid)
+    assert_same("dists", dists, od)
+    assert_same("comps", st[:, 0], oc)
