@@ -224,7 +224,21 @@ def run_profile(args, local):
         b.search(q, ids, d, st, sp)
     torch.cuda.synchronize(dev)
     stn = st.cpu().numpy()
-    print(json.dumps({"profile": True, "nq": nq, "Ls": Ls,
+    sections = None
+    if os.environ.get("PGB_LIB", "").endswith("libpgb_prof.so"):
+        # section cycles of the batched launches only: reset, run, read
+        import ctypes
+        buf = (ctypes.c_uint64 * 10)()
+        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, 10, 1))
+        for _ in range(args.steps):
+            b.search(q, ids, d, st, sp)
+        torch.cuda.synchronize(dev)
+        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, 10, 1))
+        cyc = list(buf)[:8]
+        tot = sum(cyc)
+        sections = {n: round(c / tot, 4) for n, c in zip(pgb._native.SECTION_NAMES, cyc)}
+        sections["cycles_per_expansion"] = tot / max(1, buf[8])
+    print(json.dumps({"profile": True, "nq": nq, "Ls": Ls, "sections": sections,
                       "comps": int(stn[:, 0].astype(np.int64).sum()),
                       "expansions": int(stn[:, 1].astype(np.int64).sum()),
                       "row_stride": (int(index.info.max_degree) + 31) // 32 * 32}))

@@ -128,6 +128,11 @@ pgb_status pgb_index_load_flat(int device, const char* vectors_path, pgb_elem el
 pgb_status pgb_index_load_hnsw(int device, const char* vectors_path, pgb_elem elem,
                                const char* hnsw_path, pgb_index** out);
 pgb_status pgb_index_get_info(const pgb_index* index, pgb_index_info* out);
+/* Reads and checks a file on the host only (no GPU): kind 0 = vectors, 1 = flat graph,
+ * 2 = HNSW v3 model, with the reference readers' checks (exact size / end of file, ids in
+ * range; cuda/lectores.cpp:113-187, cuda/hnsw_lector.cpp:336-419). info (may be NULL)
+ * receives {n, dim | max degree | dim, total bytes | edges | lists, 0 | 0 | entries}. */
+pgb_status pgb_file_check(const char* path, int kind, uint64_t info[4]);
 pgb_status pgb_index_destroy(pgb_index* index);
 
 /* ---- plain warp-per-query search (the drop-in) ------------------------------------ */
@@ -201,6 +206,14 @@ pgb_status pgb_batch_destroy(pgb_batch* b);
 /* recall@k with distance ties (big-ann-benchmarks compute_recall_with_distance_ties). */
 double pgb_recall(const uint32_t* gt_ids, const float* gt_dists, uint32_t nq, uint32_t gt_k,
                   const uint32_t* ids, uint32_t k);
+
+/* ---- section profiler ----------------------------------------------------------------
+ * In a library built with the section profiler (libpgb_prof.so), each flat-search warp adds
+ * the clock cycles of every search phase to device totals (the reference's -DPERFIL
+ * sections, cuda/busqueda.cuh:17-29). out receives n >= 10 counters: setup, visit,
+ * filter, distances, sort, union, shift, cut+next cycles, then expansions and queries.
+ * reset != 0 zeroes them after the read. Other builds return PGB_ERR_BAD_ARG. */
+pgb_status pgb_section_profile(uint64_t* out, uint32_t n, int reset);
 
 /* ---- graph builders (CPU, deterministic for a seed) ---------------------------------
  * vectors: n packed rows of dim bytes. nthreads <= 0: all host threads.

@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libpgb.so")
+# PGB_LIB selects another in-tree build of the same C ABI (e.g. lib/libpgb_prof.so)
+LIB_PATH = os.environ.get("PGB_LIB") or os.path.join(_HERE, "lib", "libpgb.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
@@ -89,6 +90,10 @@ _sig("pgb_build_nndescent", C.c_int, vp, u32, u32, C.c_int, u32, u32, u32, C.c_f
 _sig("pgb_build_hnsw", C.c_int, vp, u32, u32, C.c_int, u32, u32, C.c_float, C.c_float, u64,
      C.c_int, C.c_char_p)
 _sig("pgb_write_graph", C.c_int, C.c_char_p, u32, u32, vp, vp)
+_sig("pgb_section_profile", C.c_int, vp, u32, C.c_int)
+_sig("pgb_file_check", C.c_int, C.c_char_p, C.c_int, vp)
+SECTION_NAMES = ["setup", "visit", "filter", "distances", "sort", "union", "shift", "cut_next",
+                 "expansions", "queries"]
 
 
 def check(status: int) -> None:

@@ -148,6 +148,32 @@ pgb_status pgb_build_hnsw(const void* vectors, uint32_t n, uint32_t dim, pgb_ele
     return PGB_OK;
 }
 
+pgb_status pgb_file_check(const char* path, int kind, uint64_t info[4]) {
+    if (!path) return fail(PGB_ERR_BAD_ARG, "null path");
+    bool io = false;
+    std::string e;
+    uint64_t out[4] = {0, 0, 0, 0};
+    if (kind == 0) {
+        VectorFile v;
+        e = read_vectors(path, v, &io);
+        out[0] = v.n, out[1] = v.dim, out[2] = v.data.size();
+    } else if (kind == 1) {
+        GraphFile g;
+        e = read_graph(path, g, &io);
+        out[0] = g.n, out[1] = g.max_degree, out[2] = g.edges.size();
+    } else if (kind == 2) {
+        HnswFile h;
+        e = read_hnsw(path, h, &io);
+        out[0] = h.n, out[1] = h.dim, out[2] = h.list_sizes.size(), out[3] = h.entries.size();
+    } else {
+        return fail(PGB_ERR_BAD_ARG, "kind must be 0 (vectors), 1 (graph) or 2 (HNSW)");
+    }
+    if (!e.empty()) return fail(io ? PGB_ERR_IO : PGB_ERR_FORMAT, e);
+    if (info)
+        for (int i = 0; i < 4; i++) info[i] = out[i];
+    return PGB_OK;
+}
+
 pgb_status pgb_write_graph(const char* path, uint32_t n, uint32_t slots,
                            const uint32_t* degrees, const uint32_t* adjacency) {
     if (!path || !degrees || !adjacency || n == 0 || slots == 0)

@@ -14,6 +14,27 @@
 
 namespace pgb {
 
+#ifdef PGB_SECTION_PROFILE
+__device__ unsigned long long g_section_cycles[NUM_SECTIONS];
+// zero the warp's counters on entry, fold them into the device totals on exit
+#define PGB_PROF_ENTER()                                                                \
+    do {                                                                                \
+        if (lane < NUM_SECTIONS)                                                        \
+            reinterpret_cast<unsigned long long*>(wmem + A.L.off_prof)[lane] = 0ull;    \
+        __syncwarp();                                                                   \
+    } while (0)
+#define PGB_PROF_EXIT()                                                                 \
+    do {                                                                                \
+        __syncwarp();                                                                   \
+        if (lane < NUM_SECTIONS)                                                        \
+            atomicAdd(&g_section_cycles[lane],                                          \
+                      reinterpret_cast<unsigned long long*>(wmem + A.L.off_prof)[lane]); \
+    } while (0)
+#else
+#define PGB_PROF_ENTER()
+#define PGB_PROF_EXIT()
+#endif
+
 template <int CH, bool Signed, bool SFILT>
 __global__ void __launch_bounds__(128, 9) flat_plain_kernel(FlatArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -25,8 +46,10 @@ __global__ void __launch_bounds__(128, 9) flat_plain_kernel(FlatArgs A) {
     unsigned char* wmem = smem + (size_t)w * A.L.bytes;
     uint32_t* gf = A.gfilter ? A.gfilter + (size_t)gw * A.gfilter_words : nullptr;
     uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
+    PGB_PROF_ENTER();
     for (uint32_t q = gw; q < A.nq; q += total)
         flat_query<CH, Signed, SFILT>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
+    PGB_PROF_EXIT();
 }
 
 template <int CH, bool Signed, bool SFILT>
@@ -39,6 +62,7 @@ __global__ void __launch_bounds__(128, 9) flat_batched_kernel(FlatArgs A) {
     unsigned char* wmem = smem + (size_t)w * A.L.bytes;
     uint32_t* gf = A.gfilter ? A.gfilter + (size_t)gw * A.gfilter_words : nullptr;
     uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
+    PGB_PROF_ENTER();
     for (;;) {
         uint32_t slot = 0;
         if (lane == 0) slot = atomicAdd(A.queue, 1u);
@@ -47,6 +71,7 @@ __global__ void __launch_bounds__(128, 9) flat_batched_kernel(FlatArgs A) {
         const uint32_t q = A.order[slot];
         flat_query<CH, Signed, SFILT>(A, wmem, gf, gv, q, A.ls_arr[q], A.k_arr[q], lane);
     }
+    PGB_PROF_EXIT();
 }
 
 namespace {
@@ -145,3 +170,21 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
 }
 
 }  // namespace pgb
+
+extern "C" pgb_status pgb_section_profile(uint64_t* out, uint32_t n, int reset) {
+#ifdef PGB_SECTION_PROFILE
+    if (!out || n < pgb::NUM_SECTIONS) return pgb::fail(PGB_ERR_BAD_ARG, "need NUM_SECTIONS slots");
+    cudaError_t e = cudaMemcpyFromSymbol(out, pgb::g_section_cycles, 8 * pgb::NUM_SECTIONS);
+    if (e == cudaSuccess && reset) {
+        unsigned long long zero[pgb::NUM_SECTIONS] = {0};
+        e = cudaMemcpyToSymbol(pgb::g_section_cycles, zero, sizeof(zero));
+    }
+    if (e != cudaSuccess) return pgb::fail(PGB_ERR_CUDA, cudaGetErrorString(e));
+    return PGB_OK;
+#else
+    (void)out;
+    (void)n;
+    (void)reset;
+    return pgb::fail(PGB_ERR_BAD_ARG, "library built without section profiling");
+#endif
+}

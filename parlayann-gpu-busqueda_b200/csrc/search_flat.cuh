@@ -46,13 +46,54 @@ __host__ __device__ inline uint32_t flat_visited_cap(uint32_t Ls) {
     return next_pow2_u32(8u * Ls + 128u);
 }
 
+// Compile-time section profiler (build with -DPGB_SECTION_PROFILE, as the reference's
+// -DPERFIL build): each warp adds the clock64() cycles of every phase of the search to
+// counters in its shared memory and folds them into device totals when it exits.
+enum FlatSection {
+    SEC_SETUP = 0,   // query load, table clears, start point, output
+    SEC_VISIT,       // row fetch, visited marking
+    SEC_FILTER,      // lossy filter pass
+    SEC_DIST,        // distances
+    SEC_SORT,        // candidates under the cutoff, sort
+    SEC_UNION,       // multiset union decisions, visited lookups, next-row request
+    SEC_SHIFT,       // frontier shift and inserts
+    SEC_CUT_NEXT,    // cut, next unvisited, insert completion, prefetch
+    SEC_ITERATIONS,  // (count) expansions
+    SEC_QUERIES,     // (count) queries
+    NUM_SECTIONS
+};
+#ifdef PGB_SECTION_PROFILE
+constexpr uint32_t kProfileBytes = 8u * NUM_SECTIONS;
+#define PGB_PROF_BEGIN(t) long long t = clock64()
+#define PGB_PROF_ADD(sec, t)                                                  \
+    do {                                                                      \
+        const long long now_ = clock64();                                     \
+        if (lane == 0) prof[sec] += (unsigned long long)(now_ - t);           \
+        t = now_;                                                             \
+    } while (0)
+#define PGB_PROF_COUNT(sec) \
+    do {                    \
+        if (lane == 0) prof[sec] += 1ull; \
+    } while (0)
+#else
+constexpr uint32_t kProfileBytes = 0;
+#define PGB_PROF_BEGIN(t)
+#define PGB_PROF_ADD(sec, t)
+#define PGB_PROF_COUNT(sec)
+#endif
+
 struct FlatLayout {
     uint32_t ls_cap;         // frontier capacity (>= largest Ls served)
     uint32_t gs;             // adjacency row stride, multiple of 32 (>= degree limit)
     uint32_t filter_words;   // lossy filter words kept in shared memory (0: global)
     uint32_t visited_words;  // visited-table words in shared memory (0: global)
-    uint32_t off_fkey, off_fvis, off_a, off_b, off_c, off_filter, off_visited, bytes;
+    uint32_t off_fkey, off_fvis, off_a, off_b, off_c, off_vbits, off_filter, off_visited,
+        off_prof, bytes;
 };
+
+// "maybe visited" bitmap per warp: a node's bit is set when it is expanded, so a
+// candidate whose bit is clear has never been expanded and needs no table lookup
+constexpr uint32_t kVisitedBits = 1024;
 
 __host__ __device__ inline uint32_t round16(uint32_t x) { return (x + 15u) & ~15u; }
 
@@ -75,10 +116,14 @@ __host__ __device__ inline FlatLayout make_flat_layout(uint32_t ls_cap, uint32_t
     o += 8u * gs;
     L.off_c = o;  // entering positions + visited bytes
     o = round16(o + 5u * gs);
+    L.off_vbits = o;
+    o += kVisitedBits / 8u;
     L.off_filter = o;
     o += 4u * filter_words;
     L.off_visited = o;
     o += 4u * visited_words;
+    L.off_prof = o;
+    o += kProfileBytes;
     L.bytes = round16(o);
     return L;
 }
@@ -114,11 +159,10 @@ __device__ __forceinline__ uint32_t visited_home(uint32_t id, uint32_t mask) {
     return (uint32_t)(hash64_2(id) >> 32) & mask;  // reference busqueda.cu:58-60
 }
 
-// warp-cooperative insert: 32 consecutive slots per probe round, first empty wins
-__device__ __forceinline__ void visited_insert(uint32_t* tab, uint32_t mask, uint32_t id,
-                                               int lane) {
-    const uint32_t h = visited_home(id, mask);
-    for (uint32_t probe = 0; probe <= mask; probe += 32) {
+// continues an insert whose first 32 probe slots were all taken
+static __device__ __noinline__ void visited_insert_from(uint32_t* tab, uint32_t mask, uint32_t id,
+                                                 uint32_t h, int lane) {
+    for (uint32_t probe = 32; probe <= mask; probe += 32) {
         const uint32_t s = (h + probe + (uint32_t)lane) & mask;
         const uint32_t empty = __ballot_sync(kFull, tab[s] == kEmptyId);
         if (empty) {
@@ -126,12 +170,11 @@ __device__ __forceinline__ void visited_insert(uint32_t* tab, uint32_t mask, uin
             break;
         }
     }
-    __syncwarp();
 }
 
-// number of copies of id (single lane)
-__device__ __forceinline__ int visited_count(const uint32_t* tab, uint32_t mask, uint32_t id) {
-    const uint32_t h = visited_home(id, mask);
+// number of copies of id whose home slot is h (single lane)
+__device__ __forceinline__ int visited_count(const uint32_t* tab, uint32_t mask, uint32_t id,
+                                             uint32_t h) {
     int c = 0;
     for (uint32_t i = 0; i <= mask; i++) {
         const uint32_t v = tab[(h + i) & mask];
@@ -239,46 +282,66 @@ __device__ __forceinline__ void sort_keys(uint64_t* keys, int nc, int lane) {
     }
 }
 
-// ---- distances of pending rows: 8 lanes per 128-byte row, 16 rows in flight ---------
-// norm_in_row: the row's squared norm sits in bytes 124..127 (lane 7's last word)
+// ---- distances of pending rows: 4 lanes per 128-byte row, 16 rows in flight ---------
+// Lane c of a row reads its 16-byte words c and c+4, so each load instruction covers two
+// whole 32-byte sectors of 8 rows. q4: the query row (128 bytes, shared memory).
+// norm_in_row: the row's squared norm sits in bytes 124..127 (word 7, held by lane 3).
 template <bool Signed>
 __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
                                               const uint32_t* ids, int32_t* out, int np,
-                                              const int4 qv, const int32_t qq, uint32_t dim,
+                                              const int4* q4, const int32_t qq, uint32_t dim,
                                               bool norm_in_row, int lane) {
-    const int grp = lane >> 3, sub = lane & 7;
-    // bytes past dim are zero in every row; lane 7 also loads when it holds the norm
-    const bool need = (uint32_t)(sub * 16) < dim || (norm_in_row && sub == 7);
+    const int grp = lane >> 2, c = lane & 3;
+    const int4 qa = q4[c], qb = q4[c + 4];
+    // bytes past dim are zero in every row; lane 3 also loads word 7 when it holds the norm
+    const bool need_a = (uint32_t)(c * 16) < dim;
+    const bool need_b = (uint32_t)((c + 4) * 16) < dim || (norm_in_row && c == 3);
     for (int base = 0; base < np; base += 16) {
-        int4 v[4];
+        int4 va[2], vb[2];
 #pragma unroll
-        for (int r = 0; r < 4; r++) {
-            const int i = base + r * 4 + grp;
-            v[r] = make_int4(0, 0, 0, 0);
-            if (i < np && need) v[r] = ldg16(rows + (size_t)ids[i] * kRowBytes + sub * 16);
+        for (int r = 0; r < 2; r++) {
+            const int i = base + r * 8 + grp;
+            va[r] = make_int4(0, 0, 0, 0);
+            vb[r] = make_int4(0, 0, 0, 0);
+            if (i < np) {
+                const uint8_t* row = rows + (size_t)ids[i] * kRowBytes + c * 16;
+                if (need_a) va[r] = ldg16(row);
+                if (need_b) vb[r] = ldg16(row + 64);
+            }
         }
-        int32_t t[4];
+        int32_t t[2];
         if (norm_in_row) {
 #pragma unroll
-            for (int r = 0; r < 4; r++)
-                t[r] = (sub == 7 ? v[r].w : 0) - 2 * partial_dot<Signed>(v[r], qv);
+            for (int r = 0; r < 2; r++)
+                t[r] = (c == 3 ? vb[r].w : 0) -
+                       2 * (partial_dot<Signed>(va[r], qa) + partial_dot<Signed>(vb[r], qb));
         } else {
 #pragma unroll
-            for (int r = 0; r < 4; r++) t[r] = partial_l2<Signed>(v[r], qv);
+            for (int r = 0; r < 2; r++)
+                t[r] = partial_l2<Signed>(va[r], qa) + partial_l2<Signed>(vb[r], qb);
         }
 #pragma unroll
-        for (int off = 4; off > 0; off >>= 1)
+        for (int off = 2; off > 0; off >>= 1)
 #pragma unroll
-            for (int r = 0; r < 4; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 8);
-        if (sub == 0) {
+            for (int r = 0; r < 2; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 4);
+        if (c == 0) {
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int i = base + r * 4 + grp;
+            for (int r = 0; r < 2; r++) {
+                const int i = base + r * 8 + grp;
                 if (i < np) out[i] = qq + t[r];
             }
         }
     }
     __syncwarp();
+}
+
+// ||q||^2 of a zero-padded 128-byte query row, on every lane
+template <bool Signed>
+__device__ __forceinline__ int32_t query_sq_norm(const int4* q4, int lane) {
+    int32_t s = partial_sq<Signed>(q4[lane & 7]);
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) s += __shfl_xor_sync(kFull, s, off, 8);
+    return s;
 }
 
 // ---- one query -----------------------------------------------------------------------
@@ -299,6 +362,12 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     uint8_t* evis = wmem + L.off_c + 4u * L.gs;
     uint32_t* filter = SFILT ? reinterpret_cast<uint32_t*>(wmem + L.off_filter) : gfilter;
     uint32_t* vtab = gvisited ? gvisited : reinterpret_cast<uint32_t*>(wmem + L.off_visited);
+    uint32_t* vbits = reinterpret_cast<uint32_t*>(wmem + L.off_vbits);
+#ifdef PGB_SECTION_PROFILE
+    unsigned long long* prof = reinterpret_cast<unsigned long long*>(wmem + L.off_prof);
+#endif
+    PGB_PROF_BEGIN(tp);
+    PGB_PROF_COUNT(SEC_QUERIES);
 
     const uint32_t qid = A.qbase + q;
     const uint32_t fmask = (1u << flat_filter_bits(Ls)) - 1u;
@@ -317,18 +386,17 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         for (uint32_t i = lane; i < (fmask + 1u) / 4u; i += 32) f4[i] = e4;
         uint4* v4 = reinterpret_cast<uint4*>(vtab);
         for (uint32_t i = lane; i < vcap / 4u; i += 32) v4[i] = e4;
+        if (lane < (int)(kVisitedBits / 128u)) reinterpret_cast<uint4*>(vbits)[lane] = make_uint4(0, 0, 0, 0);
     }
     __syncwarp();
-    const int4 qv = reinterpret_cast<const int4*>(qwords)[lane & 7];
-    int32_t qq = partial_sq<Signed>(qv);
-#pragma unroll
-    for (int off = 4; off > 0; off >>= 1) qq += __shfl_xor_sync(kFull, qq, off, 8);
+    const int4* q4 = reinterpret_cast<const int4*>(qwords);
+    const int32_t qq = query_sq_norm<Signed>(q4, lane);
 
     // start point: F = {(d(q, start), start)}, one distance
     if (lane == 0) pend[0] = A.start;
     __syncwarp();
     const bool nir = A.norm_in_row != 0;
-    row_distances<Signed>(A.rows, pend, pdist, 1, qv, qq, A.dim, nir, lane);
+    row_distances<Signed>(A.rows, pend, pdist, 1, q4, qq, A.dim, nir, lane);
     if (lane == 0) {
         fkey[0] = pack_key(pdist[0], A.start);
         fvis[0] = 0;
@@ -344,7 +412,9 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     uint32_t apred[CH];
     int u2 = -1;  // second unvisited frontier entry when known
 
+    PGB_PROF_ADD(SEC_SETUP, tp);
     while (u >= 0 && (int64_t)nvis < limit) {
+        PGB_PROF_COUNT(SEC_ITERATIONS);
         const uint64_t cur_key = fkey[u];
         const uint32_t cur = key_id(cur_key);
         // whole neighbour row: the predicted one, or requested now
@@ -361,13 +431,24 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
             }
         }
         if (lane == 0) fvis[u] = 1;
-        visited_insert(vtab, vmask, cur, lane);
+        // visited insert of cur, in two halves: the 32 probe slots are read now and the
+        // slot is claimed at the end of the iteration (only this warp writes the table);
+        // lookups in between add the pending copy themselves
+        const uint64_t hcur = hash64_2(cur);
+        const uint32_t vhome = (uint32_t)(hcur >> 32) & vmask;
+        const uint32_t vslot = (vhome + (uint32_t)lane) & vmask;
+        const uint32_t vprobe = vtab[vslot];
+        if (lane == 0) {
+            const uint32_t b = (uint32_t)(hcur >> 48) & (kVisitedBits - 1u);
+            vbits[b >> 5] |= 1u << (b & 31u);
+        }
         nvis++;
         if (nvis > max_visits) {
             flags |= PGB_FLAG_OVERFLOW;
             break;
         }
         const int32_t cutoff = (fsize < (int)Ls) ? INT_MAX : key_dist(fkey[fsize - 1]);
+        PGB_PROF_ADD(SEC_VISIT, tp);
 
         // ---- lossy filter in row order -> pending ids ------------------------------
         int np = 0;
@@ -441,9 +522,11 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
             }
         }
         comps += np;
+        PGB_PROF_ADD(SEC_FILTER, tp);
 
         // ---- distances ------------------------------------------------------------
-        row_distances<Signed>(A.rows, pend, pdist, np, qv, qq, A.dim, nir, lane);
+        row_distances<Signed>(A.rows, pend, pdist, np, q4, qq, A.dim, nir, lane);
+        PGB_PROF_ADD(SEC_DIST, tp);
 
         // ---- candidates under the cutoff, in arrival order ------------------------
         int nc = 0;
@@ -464,6 +547,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         int ne = 0;
         if (nc > 0) {
             sort_keys<CH>(ckey, nc, lane);
+            PGB_PROF_ADD(SEC_SORT, tp);
             // ---- multiset set_union: copy `rep` of a key enters iff rep >= copies in F
             for (int base = 0; base < nc; base += 32) {
                 const int i = base + lane;
@@ -479,8 +563,16 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                     int rep = 0;
                     while (i - rep - 1 >= 0 && ckey[i - rep - 1] == key) rep++;
                     enter = rep >= cf;
-                    if (enter)
-                        vis = (uint8_t)(rep < visited_count(vtab, vmask, key_id(key)));
+                    if (enter) {
+                        const uint32_t id = key_id(key);
+                        const uint64_t hh = hash64_2(id);
+                        const uint32_t b = (uint32_t)(hh >> 48) & (kVisitedBits - 1u);
+                        int cnt = 0;
+                        if ((vbits[b >> 5] >> (b & 31u)) & 1u)
+                            cnt = visited_count(vtab, vmask, id, (uint32_t)(hh >> 32) & vmask) +
+                                  (id == cur ? 1 : 0);
+                        vis = (uint8_t)(rep < cnt);
+                    }
                 }
                 const uint32_t m = __ballot_sync(kFull, enter);
                 // new copies follow the frontier copies of an equal key
@@ -513,6 +605,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 apred[t] = (j < deg_lim) ? __ldg(prow + j) : kEmptyId;
             }
         }
+        PGB_PROF_ADD(SEC_UNION, tp);
         {
             if (ne > 0) {
                 // the expanded entry's new position, then shift the frontier tail
@@ -545,6 +638,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 fsize = min((int)Ls, fsize + ne);
             }
         }
+        PGB_PROF_ADD(SEC_SHIFT, tp);
 
         // ---- cut --------------------------------------------------------------------
         if (fsize > (int)k) {
@@ -584,6 +678,15 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 break;
             }
         }
+        // second half of the visited insert
+        {
+            const uint32_t empty = __ballot_sync(kFull, vprobe == kEmptyId);
+            if (empty) {
+                if (lane == __ffs(empty) - 1) vtab[vslot] = cur;
+            } else {
+                visited_insert_from(vtab, vmask, cur, vhome, lane);
+            }
+        }
         // the prediction held: pull the vector rows of its neighbours into L2 now, ahead
         // of the next distance phase (rows the filter will drop are fetched too)
         if (u >= 0 && key_id(fkey[u]) == pred) {
@@ -592,6 +695,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 if (apred[t] != kEmptyId) prefetch_row_l2(A.rows + (size_t)apred[t] * kRowBytes);
         }
         __syncwarp();
+        PGB_PROF_ADD(SEC_CUT_NEXT, tp);
     }
 
     // ---- output: first k of the frontier ----------------------------------------------
@@ -613,6 +717,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         A.stats[q] = s;
     }
     __syncwarp();
+    PGB_PROF_ADD(SEC_SETUP, tp);
 }
 
 }  // namespace pgb

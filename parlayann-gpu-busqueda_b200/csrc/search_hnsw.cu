@@ -161,10 +161,8 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
     for (uint32_t q = gw; q < A.nq; q += total) {
         load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
         __syncwarp();
-        const int4 qv = reinterpret_cast<const int4*>(qwords)[lane & 7];
-        int32_t qq = partial_sq<Signed>(qv);
-#pragma unroll
-        for (int off = 4; off > 0; off >>= 1) qq += __shfl_xor_sync(kFull, qq, off, 8);
+        const int4* q4 = reinterpret_cast<const int4*>(qwords);
+        const int32_t qq = query_sq_norm<Signed>(q4, lane);
 
         int comps = 0, exps = 0, flags = 0;
         int neps = (int)A.n_entries;
@@ -189,7 +187,7 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
             // ---- entry points: distances, then the sequential inserts on lane 0 ----
             for (int e = lane; e < neps; e += 32) pend[e] = eps[e];
             __syncwarp();
-            row_distances<Signed>(A.rows, pend, pd, neps, qv, qq, A.dim, A.norm_in_row != 0, lane);
+            row_distances<Signed>(A.rows, pend, pd, neps, q4, qq, A.dim, A.norm_in_row != 0, lane);
             int nC = 0;
             nW = 0;
             if (lane == 0) {
@@ -314,7 +312,7 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
                     }
                 }
                 comps += np;
-                row_distances<Signed>(A.rows, pend, pd, np, qv, qq, A.dim, A.norm_in_row != 0, lane);
+                row_distances<Signed>(A.rows, pend, pd, np, q4, qq, A.dim, A.norm_in_row != 0, lane);
 
                 // ---- eligibility: first copy in this expansion and not in is_inw ------
                 for (int j = lane; j < np; j += 32) {

@@ -17,8 +17,11 @@ struct FlatPlanRequest {
     bool batched = false;
     int warps_per_block = 0;       // 0: default (4)
     int max_blocks_per_sm = 0;     // 0: as many as fit
-    uint32_t filter_smem_limit = 16384;   // bytes: filter in shared memory up to this
-    uint32_t visited_smem_limit = 8192;   // bytes: visited table in shared memory up to this
+    // table placement: the lossy filter is read on every neighbour and stays in shared
+    // memory up to 16 KB; the visited table is touched once per expansion and lives in
+    // global memory (L2), which keeps more warps resident
+    uint32_t filter_smem_limit = 16384;
+    uint32_t visited_smem_limit = 0;
     bool force_filter_placement = false;
     bool filter_in_shared = true;
     bool force_visited_placement = false;

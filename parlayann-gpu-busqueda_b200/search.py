@@ -219,6 +219,15 @@ def build_hnsw(x: np.ndarray, path: str, M: int = 32, ef_construction: int = 128
                                  ef_construction, ml, alpha, seed, threads, path.encode()))
 
 
+def file_check(path: str, kind: str):
+    """C-reader validation of a file on the host: kind 'vectors', 'graph' or 'hnsw'.
+    Returns the 4 info counters; raises PgbError (IO or FORMAT) on a bad file."""
+    info = (C.c_uint64 * 4)()
+    k = {"vectors": 0, "graph": 1, "hnsw": 2}[kind]
+    N.check(N.lib.pgb_file_check(path.encode(), k, info))
+    return list(info)
+
+
 def device_available() -> bool:
     return bool(N.lib.pgb_device_available())
 
