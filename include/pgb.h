@@ -202,6 +202,47 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t query_s
 pgb_status pgb_batch_replay(pgb_batch* b, void* stream);
 pgb_status pgb_batch_destroy(pgb_batch* b);
 
+/* ---- serving (no counterpart in the reference) ----------------------------------------
+ * A request loop over one flat-graph index. submit() copies the query and admits the
+ * request into a bounded pool (PGB_ERR_BUSY when full; the pool is sized by the device
+ * memory budget). A dispatcher thread continuously packs whatever has arrived into
+ * batches (longest beam first) and launches them on up to max_inflight streams, so
+ * requests that arrive while others are on the GPU start as soon as a stream and slots
+ * free up, overlapping with them. Each request gets exactly the neighbours that
+ * pgb_searcher_search returns for it alone with the same params (exclusion quirk off). */
+typedef struct pgb_server_options {
+    uint32_t max_beam;       /* largest beam a request may ask for                       */
+    uint32_t max_k;          /* largest k a request may ask for                          */
+    uint32_t max_batch;      /* requests per launch (0: 1024)                            */
+    uint32_t max_inflight;   /* launches on the GPU at once (0: 4)                       */
+    uint64_t memory_budget;  /* device bytes for the pool (0: half of the free memory)   */
+    double cut;              /* as pgb_query_params                                      */
+    int64_t limit;
+    uint32_t degree_limit;
+    uint32_t max_wait_us;    /* hold a partial batch at most this long while launches are
+                                in flight, to grow it (0: launch at once)                */
+} pgb_server_options;
+
+typedef struct pgb_server_stats {
+    uint64_t submitted, completed, rejected, launches;
+    uint32_t pending, in_flight, pool_slots, streams;
+    double p50_us, p99_us;   /* submit-to-completion latency over the last 65,536 requests */
+    double mean_batch;       /* requests per launch                                         */
+} pgb_server_stats;
+
+pgb_status pgb_server_create(pgb_index* index, const pgb_server_options* opt,
+                             pgb_server** out);
+/* query: host memory, index dim bytes; the ticket names the request in poll() */
+pgb_status pgb_server_submit(pgb_server* s, const void* query, uint32_t beam_size, uint32_t k,
+                             uint64_t* ticket);
+/* Waits up to timeout_us for the request; PGB_ERR_TIMEOUT if it is not done yet. On
+ * success copies k ids / dists (and stats, may be NULL) and releases the ticket. */
+pgb_status pgb_server_poll(pgb_server* s, uint64_t ticket, uint32_t timeout_us, uint32_t* ids,
+                           int32_t* dists, pgb_query_stats* stats);
+pgb_status pgb_server_get_stats(pgb_server* s, pgb_server_stats* out);
+/* completes the requests in flight, then frees everything */
+pgb_status pgb_server_destroy(pgb_server* s);
+
 /* ---- evaluation ---------------------------------------------------------------- */
 /* recall@k with distance ties (big-ann-benchmarks compute_recall_with_distance_ties). */
 double pgb_recall(const uint32_t* gt_ids, const float* gt_dists, uint32_t nq, uint32_t gt_k,

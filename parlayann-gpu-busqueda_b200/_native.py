@@ -125,3 +125,23 @@ _sig("pgb_batch_get_config", C.c_int, vp, C.POINTER(BatchConfig))
 _sig("pgb_batch_capture", C.c_int, vp, vp, u32, vp, vp, vp)
 _sig("pgb_batch_replay", C.c_int, vp, vp)
 _sig("pgb_batch_destroy", C.c_int, vp)
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [("max_beam", C.c_uint32), ("max_k", C.c_uint32), ("max_batch", C.c_uint32),
+                ("max_inflight", C.c_uint32), ("memory_budget", C.c_uint64), ("cut", C.c_double),
+                ("limit", C.c_int64), ("degree_limit", C.c_uint32), ("max_wait_us", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("rejected", C.c_uint64),
+                ("launches", C.c_uint64), ("pending", C.c_uint32), ("in_flight", C.c_uint32),
+                ("pool_slots", C.c_uint32), ("streams", C.c_uint32), ("p50_us", C.c_double),
+                ("p99_us", C.c_double), ("mean_batch", C.c_double)]
+
+
+_sig("pgb_server_create", C.c_int, vp, C.POINTER(ServerOptions), C.POINTER(vp))
+_sig("pgb_server_submit", C.c_int, vp, vp, u32, u32, C.POINTER(C.c_uint64))
+_sig("pgb_server_poll", C.c_int, vp, C.c_uint64, u32, vp, vp, vp)
+_sig("pgb_server_get_stats", C.c_int, vp, C.POINTER(ServerStats))
+_sig("pgb_server_destroy", C.c_int, vp)

@@ -162,8 +162,12 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
     A.gfilter_words = P.gfilter_words;
     A.gvisited_words = P.gvisited_words;
     void* args[] = {&A};
-    cudaError_t e = cudaLaunchKernel(P.kernel, dim3(P.blocks), dim3(P.warps_per_block * 32),
-                                     args, P.smem_bytes, stream);
+    // the work-queue form needs no more warps than queries (small serving batches)
+    int blocks = P.blocks;
+    if (P.batched)
+        blocks = std::max(1, std::min(blocks, (int)((A.nq + P.warps_per_block - 1) / P.warps_per_block)));
+    cudaError_t e = cudaLaunchKernel(P.kernel, dim3(blocks), dim3(P.warps_per_block * 32), args,
+                                     P.smem_bytes, stream);
     if (e != cudaSuccess)
         return fail(PGB_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
     return PGB_OK;

@@ -1,0 +1,472 @@
+// server.cu -- pgb_server_*: a continuous-batching request loop over a flat-graph index.
+//
+// Host side: submit() admits a request into a bounded slot pool (busy when full) and
+// wakes the dispatcher thread. The dispatcher completes finished launches (event query),
+// then packs the pending requests into batches -- longest beam first -- and launches each
+// on a free stream context: one upload of the packed queries and per-request (Ls, k),
+// one work-queue launch of the batched kernel (the grid shrinks to the batch), one
+// download per output array. New arrivals therefore start while earlier launches are
+// still on the GPU, and their work overlaps on the device. Every request runs the same
+// per-query code as the plain searcher, so its answer does not depend on the mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "errors.h"
+#include "index.h"
+#include "search_plan.h"
+#include "searcher.h"
+
+namespace pgb {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Slot {
+    uint64_t ticket = 0;
+    uint32_t Ls = 0, k = 0;
+    Clock::time_point t_submit;
+    bool done = false;
+    std::vector<uint8_t> query;
+    std::vector<uint32_t> ids;
+    std::vector<int32_t> dists;
+    pgb_query_stats stats{};
+};
+
+// one launch on its own stream
+struct Context {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    bool busy = false;
+    std::vector<uint32_t> slots;  // pool slots, batch-local order
+    uint8_t* h_in = nullptr;      // pinned: queries | ls | k | order
+    uint32_t* h_ids = nullptr;
+    int32_t* h_dists = nullptr;
+    pgb_query_stats* h_stats = nullptr;
+    uint8_t* d_in = nullptr;
+    uint32_t* d_ids = nullptr;
+    int32_t* d_dists = nullptr;
+    pgb_query_stats* d_stats = nullptr;
+    uint32_t* d_queue = nullptr;
+    uint32_t* gfilter = nullptr;
+    uint32_t* gvisited = nullptr;
+};
+
+constexpr size_t kLatencyRing = 65536;
+
+}  // namespace
+}  // namespace pgb
+
+struct pgb_server {
+    pgb_index* index = nullptr;
+    pgb_server_options opt{};
+    pgb::FlatPlan plan{};
+    uint32_t deg_lim = 0;
+    size_t in_q_bytes = 0, in_bytes = 0;  // staging layout
+    std::vector<pgb::Context> ctx;
+    std::vector<pgb::Slot> pool;
+    std::vector<uint32_t> free_slots;
+    std::deque<uint32_t> pending;
+    std::unordered_map<uint64_t, uint32_t> by_ticket;
+    uint64_t next_ticket = 1;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread dispatcher;
+    bool stop = false;
+    pgb_status failed = PGB_OK;
+    std::string fail_msg;
+    uint64_t submitted = 0, completed = 0, rejected = 0, launches = 0, launched_requests = 0;
+    std::vector<float> lat_us;
+    size_t lat_pos = 0;
+    bool lat_full = false;
+};
+
+namespace pgb {
+namespace {
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+void free_context(Context& c) {
+    if (c.stream) cudaStreamDestroy(c.stream);
+    if (c.done) cudaEventDestroy(c.done);
+    cudaFreeHost(c.h_in);
+    cudaFreeHost(c.h_ids);
+    cudaFreeHost(c.h_dists);
+    cudaFreeHost(c.h_stats);
+    cudaFree(c.d_in);
+    cudaFree(c.d_ids);
+    cudaFree(c.d_dists);
+    cudaFree(c.d_stats);
+    cudaFree(c.d_queue);
+    cudaFree(c.gfilter);
+    cudaFree(c.gvisited);
+    c = Context{};
+}
+
+pgb_status alloc_context(pgb_server* S, Context& c) {
+    const size_t mb = S->opt.max_batch, mk = S->opt.max_k;
+    pgb_status s;
+    if ((s = cuda_status(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking), "stream")) != PGB_OK ||
+        (s = cuda_status(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming), "event")) != PGB_OK ||
+        (s = cuda_status(cudaMallocHost(&c.h_in, S->in_bytes), "pinned staging")) != PGB_OK ||
+        (s = cuda_status(cudaMallocHost(&c.h_ids, 4 * mb * mk), "pinned staging")) != PGB_OK ||
+        (s = cuda_status(cudaMallocHost(&c.h_dists, 4 * mb * mk), "pinned staging")) != PGB_OK ||
+        (s = cuda_status(cudaMallocHost(&c.h_stats, sizeof(pgb_query_stats) * mb), "pinned staging")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&c.d_in, S->in_bytes), "device staging")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&c.d_ids, 4 * mb * mk), "device outputs")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&c.d_dists, 4 * mb * mk), "device outputs")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&c.d_stats, sizeof(pgb_query_stats) * mb), "device outputs")) != PGB_OK ||
+        (s = cuda_status(cudaMalloc(&c.d_queue, 4), "queue counter")) != PGB_OK)
+        return s;
+    const uint64_t tw = S->plan.total_warps;
+    if (S->plan.gfilter_words &&
+        (s = cuda_status(cudaMalloc(&c.gfilter, 4ull * S->plan.gfilter_words * tw), "filter scratch")) != PGB_OK)
+        return s;
+    if (S->plan.gvisited_words &&
+        (s = cuda_status(cudaMalloc(&c.gvisited, 4ull * S->plan.gvisited_words * tw), "visited scratch")) != PGB_OK)
+        return s;
+    return PGB_OK;
+}
+
+size_t context_device_bytes(const pgb_server* S) {
+    const size_t mb = S->opt.max_batch, mk = S->opt.max_k, tw = S->plan.total_warps;
+    return S->in_bytes + 8 * mb * mk + sizeof(pgb_query_stats) * mb + 4 +
+           4ull * (S->plan.gfilter_words + S->plan.gvisited_words) * tw;
+}
+
+void set_failed(pgb_server* S, pgb_status s, const std::string& m) {
+    if (S->failed == PGB_OK) {
+        S->failed = s;
+        S->fail_msg = m;
+    }
+    S->cv_done.notify_all();
+}
+
+// called with the lock held
+void launch(pgb_server* S, Context& c) {
+    const pgb_index* ix = S->index;
+    const size_t mb = S->opt.max_batch;
+    const uint32_t b = (uint32_t)std::min<size_t>(mb, S->pending.size());
+    c.slots.assign(S->pending.begin(), S->pending.begin() + b);
+    S->pending.erase(S->pending.begin(), S->pending.begin() + b);
+    uint32_t* ls = reinterpret_cast<uint32_t*>(c.h_in + S->in_q_bytes);
+    uint32_t* ks = ls + mb;
+    uint32_t* order = ks + mb;
+    for (uint32_t j = 0; j < b; j++) {
+        const Slot& sl = S->pool[c.slots[j]];
+        memcpy(c.h_in + (size_t)j * ix->dim, sl.query.data(), ix->dim);
+        ls[j] = sl.Ls;
+        ks[j] = sl.k;
+        order[j] = j;
+    }
+    std::stable_sort(order, order + b, [&](uint32_t a, uint32_t d) { return ls[a] > ls[d]; });
+    cudaError_t e = cudaMemcpyAsync(c.d_in, c.h_in, S->in_bytes, cudaMemcpyHostToDevice, c.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d_queue, 0, 4, c.stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_failed(S, PGB_ERR_CUDA, std::string("server upload: ") + cudaGetErrorString(e));
+        return;
+    }
+    FlatArgs A{};
+    A.rows = ix->rows;
+    A.adj = ix->adj;
+    A.n = ix->n;
+    A.gs = ix->gs;
+    A.deg_lim = S->deg_lim;
+    A.dim = ix->dim;
+    A.start = 0;
+    A.queries = c.d_in;
+    A.nq = b;
+    A.qstride = ix->dim;
+    A.cut = S->opt.cut;
+    A.limit = S->opt.limit <= 0 ? (int64_t)ix->n : S->opt.limit;
+    A.excl = 0;
+    A.qbase = 0;
+    A.norm_in_row = ix->norm_in_row ? 1u : 0u;
+    A.ls_arr = reinterpret_cast<const uint32_t*>(c.d_in + S->in_q_bytes);
+    A.k_arr = A.ls_arr + mb;
+    A.order = A.k_arr + mb;
+    A.out_stride = S->opt.max_k;
+    A.ids = c.d_ids;
+    A.dists = c.d_dists;
+    A.stats = c.d_stats;
+    A.gfilter = c.gfilter;
+    A.gvisited = c.gvisited;
+    A.queue = c.d_queue;
+    if (launch_flat(S->plan, A, c.stream) != PGB_OK) {
+        set_failed(S, PGB_ERR_CUDA, pgb_last_error());
+        return;
+    }
+    const size_t mk = S->opt.max_k;
+    e = cudaMemcpyAsync(c.h_ids, c.d_ids, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c.h_dists, c.d_dists, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c.h_stats, c.d_stats, sizeof(pgb_query_stats) * b,
+                            cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_failed(S, PGB_ERR_CUDA, std::string("server launch: ") + cudaGetErrorString(e));
+        return;
+    }
+    c.busy = true;
+    S->launches++;
+    S->launched_requests += b;
+}
+
+// called with the lock held
+void finish(pgb_server* S, Context& c) {
+    const size_t mk = S->opt.max_k;
+    const auto now = Clock::now();
+    for (size_t j = 0; j < c.slots.size(); j++) {
+        Slot& sl = S->pool[c.slots[j]];
+        std::copy(c.h_ids + j * mk, c.h_ids + j * mk + sl.k, sl.ids.begin());
+        std::copy(c.h_dists + j * mk, c.h_dists + j * mk + sl.k, sl.dists.begin());
+        sl.stats = c.h_stats[j];
+        sl.done = true;
+        const float us = std::chrono::duration<float, std::micro>(now - sl.t_submit).count();
+        S->lat_us[S->lat_pos] = us;
+        S->lat_pos = (S->lat_pos + 1) % kLatencyRing;
+        if (S->lat_pos == 0) S->lat_full = true;
+        S->completed++;
+    }
+    c.slots.clear();
+    c.busy = false;
+    S->cv_done.notify_all();
+}
+
+void dispatch_loop(pgb_server* S) {
+    cudaSetDevice(S->index->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        bool progressed = false;
+        int inflight = 0;
+        for (Context& c : S->ctx) {
+            if (!c.busy) continue;
+            const cudaError_t q = cudaEventQuery(c.done);
+            if (q == cudaSuccess) {
+                finish(S, c);
+                progressed = true;
+            } else if (q != cudaErrorNotReady) {
+                cudaGetLastError();
+                set_failed(S, PGB_ERR_CUDA, std::string("server kernel: ") + cudaGetErrorString(q));
+                c.busy = false;
+            } else {
+                inflight++;
+            }
+        }
+        if (S->failed == PGB_OK) {
+            for (Context& c : S->ctx) {
+                if (c.busy || S->pending.empty()) continue;
+                // while other launches run, a partial batch may wait a little to grow
+                if (inflight > 0 && S->opt.max_wait_us > 0 && S->pending.size() < S->opt.max_batch) {
+                    const auto age = Clock::now() - S->pool[S->pending.front()].t_submit;
+                    if (age < std::chrono::microseconds(S->opt.max_wait_us)) break;
+                }
+                launch(S, c);
+                if (S->failed != PGB_OK) break;
+                inflight++;
+                progressed = true;
+            }
+        }
+        if (S->stop && (S->pending.empty() || S->failed != PGB_OK) && inflight == 0) break;
+        if (!progressed) {
+            if (inflight > 0) {
+                lk.unlock();
+                std::this_thread::yield();
+                lk.lock();
+            } else {
+                S->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            }
+        }
+    }
+}
+
+void destroy_server(pgb_server* S) {
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    if (S->dispatcher.joinable()) S->dispatcher.join();
+    DeviceGuard g(S->index->device);
+    for (Context& c : S->ctx) {
+        if (c.stream) cudaStreamSynchronize(c.stream);
+        free_context(c);
+    }
+    delete S;
+}
+
+}  // namespace
+}  // namespace pgb
+
+using namespace pgb;
+
+extern "C" {
+
+pgb_status pgb_server_create(pgb_index* ix, const pgb_server_options* opt, pgb_server** out) {
+    if (!out) return fail(PGB_ERR_BAD_ARG, "null output handle");
+    *out = nullptr;
+    if (!ix || !opt) return fail(PGB_ERR_BAD_ARG, "null index or options");
+    if (ix->is_hnsw) return fail(PGB_ERR_BAD_ARG, "the server serves flat graphs");
+    if (opt->max_beam == 0 || opt->max_beam > PGB_MAX_BEAM || opt->max_k == 0 ||
+        opt->max_k > PGB_MAX_K || !(opt->cut > 0))
+        return fail(PGB_ERR_BAD_ARG, "bad max_beam / max_k / cut");
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    pgb_server* S = new pgb_server();
+    S->index = ix;
+    S->opt = *opt;
+    if (S->opt.max_batch == 0) S->opt.max_batch = 1024;
+    if (S->opt.max_inflight == 0) S->opt.max_inflight = 4;
+    S->deg_lim = opt->degree_limit ? std::min(opt->degree_limit, ix->G) : ix->G;
+    FlatPlanRequest rq;
+    rq.max_ls = S->opt.max_beam;
+    rq.deg_lim = S->deg_lim;
+    rq.is_signed = ix->elem == PGB_INT8;
+    rq.batched = true;
+    pgb_status s = plan_flat(rq, S->plan);
+    if (s != PGB_OK) {
+        delete S;
+        return s;
+    }
+    const size_t mb = S->opt.max_batch;
+    S->in_q_bytes = align16(mb * ix->dim);
+    S->in_bytes = S->in_q_bytes + 12 * mb;
+    // admission by free memory: as many stream contexts as the budget holds
+    size_t free_b = 0, total_b = 0;
+    if ((s = cuda_status(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo")) != PGB_OK) {
+        delete S;
+        return s;
+    }
+    const size_t budget = S->opt.memory_budget ? S->opt.memory_budget : free_b / 2;
+    const size_t per = context_device_bytes(S);
+    const size_t fit = per ? budget / per : 0;
+    if (fit == 0) {
+        delete S;
+        return fail(PGB_ERR_OOM, "memory budget below one launch context");
+    }
+    S->ctx.resize(std::min<size_t>(S->opt.max_inflight, fit));
+    for (Context& c : S->ctx)
+        if ((s = alloc_context(S, c)) != PGB_OK) {
+            for (Context& d : S->ctx) free_context(d);
+            delete S;
+            return s;
+        }
+    // pool: every context's batch in flight plus as many waiting
+    const size_t slots = 2 * S->ctx.size() * mb;
+    S->pool.resize(slots);
+    for (Slot& sl : S->pool) {
+        sl.query.resize(ix->dim);
+        sl.ids.resize(S->opt.max_k);
+        sl.dists.resize(S->opt.max_k);
+    }
+    S->free_slots.resize(slots);
+    std::iota(S->free_slots.rbegin(), S->free_slots.rend(), 0u);
+    S->lat_us.assign(kLatencyRing, 0.f);
+    S->dispatcher = std::thread(dispatch_loop, S);
+    *out = S;
+    return PGB_OK;
+}
+
+pgb_status pgb_server_submit(pgb_server* S, const void* query, uint32_t beam_size, uint32_t k,
+                             uint64_t* ticket) {
+    if (!S || !query || !ticket) return fail(PGB_ERR_BAD_ARG, "null argument");
+    if (beam_size == 0 || beam_size > S->opt.max_beam) return fail(PGB_ERR_BAD_ARG, "beam size outside 1..max_beam");
+    if (k == 0 || k > S->opt.max_k) return fail(PGB_ERR_BAD_ARG, "k outside 1..max_k");
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->failed != PGB_OK) return fail(S->failed, S->fail_msg);
+        if (S->stop) return fail(PGB_ERR_BAD_ARG, "server is shutting down");
+        if (S->free_slots.empty()) {
+            S->rejected++;
+            return fail(PGB_ERR_BUSY, "request pool full");
+        }
+        const uint32_t slot = S->free_slots.back();
+        S->free_slots.pop_back();
+        Slot& sl = S->pool[slot];
+        memcpy(sl.query.data(), query, S->index->dim);
+        sl.Ls = beam_size;
+        sl.k = k;
+        sl.done = false;
+        sl.ticket = S->next_ticket++;
+        sl.t_submit = Clock::now();
+        S->by_ticket[sl.ticket] = slot;
+        S->pending.push_back(slot);
+        S->submitted++;
+        *ticket = sl.ticket;
+    }
+    S->cv_work.notify_one();
+    return PGB_OK;
+}
+
+pgb_status pgb_server_poll(pgb_server* S, uint64_t ticket, uint32_t timeout_us, uint32_t* ids,
+                           int32_t* dists, pgb_query_stats* stats) {
+    if (!S || !ids || !dists) return fail(PGB_ERR_BAD_ARG, "null argument");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->by_ticket.find(ticket);
+    if (it == S->by_ticket.end()) return fail(PGB_ERR_NOT_FOUND, "unknown ticket");
+    const uint32_t slot = it->second;
+    Slot& sl = S->pool[slot];
+    if (!sl.done) {
+        S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us),
+                            [&] { return sl.done || S->failed != PGB_OK; });
+    }
+    if (!sl.done) {
+        if (S->failed != PGB_OK) return fail(S->failed, S->fail_msg);
+        return fail(PGB_ERR_TIMEOUT, "request not finished");
+    }
+    std::copy(sl.ids.begin(), sl.ids.begin() + sl.k, ids);
+    std::copy(sl.dists.begin(), sl.dists.begin() + sl.k, dists);
+    if (stats) *stats = sl.stats;
+    S->by_ticket.erase(it);
+    S->free_slots.push_back(slot);
+    return PGB_OK;
+}
+
+pgb_status pgb_server_get_stats(pgb_server* S, pgb_server_stats* out) {
+    if (!S || !out) return fail(PGB_ERR_BAD_ARG, "null argument");
+    std::vector<float> lat;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        out->submitted = S->submitted;
+        out->completed = S->completed;
+        out->rejected = S->rejected;
+        out->launches = S->launches;
+        out->pending = (uint32_t)S->pending.size();
+        uint32_t inflight = 0;
+        for (const Context& c : S->ctx) inflight += c.busy ? (uint32_t)c.slots.size() : 0u;
+        out->in_flight = inflight;
+        out->pool_slots = (uint32_t)S->pool.size();
+        out->streams = (uint32_t)S->ctx.size();
+        out->mean_batch = S->launches ? (double)S->launched_requests / S->launches : 0.0;
+        const size_t n = S->lat_full ? kLatencyRing : S->lat_pos;
+        lat.assign(S->lat_us.begin(), S->lat_us.begin() + n);
+    }
+    out->p50_us = out->p99_us = 0;
+    if (!lat.empty()) {
+        const size_t i50 = lat.size() / 2, i99 = std::min(lat.size() - 1, lat.size() * 99 / 100);
+        std::nth_element(lat.begin(), lat.begin() + i50, lat.end());
+        out->p50_us = lat[i50];
+        std::nth_element(lat.begin(), lat.begin() + i99, lat.end());
+        out->p99_us = lat[i99];
+    }
+    return PGB_OK;
+}
+
+pgb_status pgb_server_destroy(pgb_server* S) {
+    if (!S) return PGB_OK;
+    destroy_server(S);
+    return PGB_OK;
+}
+
+}  // extern "C"

@@ -315,3 +315,57 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Server:
+    """Continuous-batching request loop (pgb_server_*): submit() -> ticket, poll(ticket)."""
+
+    BUSY, TIMEOUT = 7, 8
+
+    def __init__(self, index: Index, max_beam: int, max_k: int, max_batch: int = 0,
+                 max_inflight: int = 0, memory_budget: int = 0, cut: float = 1.35,
+                 limit: int = 0, degree_limit: int = 0, max_wait_us: int = 0):
+        self.index, self.max_k = index, max_k
+        self._opt = N.ServerOptions(max_beam, max_k, max_batch, max_inflight, memory_budget,
+                                    float(cut), int(limit), degree_limit, max_wait_us)
+        h = C.c_void_p()
+        N.check(N.lib.pgb_server_create(index.handle, C.byref(self._opt), C.byref(h)))
+        self._h = h
+
+    def submit(self, query: np.ndarray, beam_size: int, k: int):
+        """Returns the ticket, or None when the pool is full (PGB_ERR_BUSY)."""
+        q = np.ascontiguousarray(query)
+        t = C.c_uint64()
+        st = N.lib.pgb_server_submit(self._h, _ptr(q), beam_size, k, C.byref(t))
+        if st == self.BUSY:
+            return None
+        N.check(st)
+        return t.value
+
+    def poll(self, ticket: int, k: int, timeout_us: int = 0):
+        """(ids, dists, stats) when done, None on timeout."""
+        ids = np.empty(k, np.uint32)
+        dists = np.empty(k, np.int32)
+        stats = np.empty(4, np.int32)
+        st = N.lib.pgb_server_poll(self._h, ticket, timeout_us, _ptr(ids), _ptr(dists),
+                                   _ptr(stats))
+        if st == self.TIMEOUT:
+            return None
+        N.check(st)
+        return ids, dists, stats
+
+    def stats(self) -> dict:
+        s = N.ServerStats()
+        N.check(N.lib.pgb_server_get_stats(self._h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in N.ServerStats._fields_}
+
+    def close(self):
+        if self._h:
+            N.lib.pgb_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
