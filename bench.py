@@ -56,29 +56,58 @@ def dist_env():
     return rank, world, local
 
 
-def load_workload(pgb, rank, barrier):
-    """Base vectors, this rank's queries and the Vamana graph (cached on disk)."""
+# the four graph families of the 1M workload, as the reference's runs name them
+GRAPHS = {
+    "vamana": ("c2_vamana_R64_L128_a1.2.graph", "Vamana R64 L128 alpha1.2",
+               lambda pgb, x: pgb.build_vamana(x, R=R, L=L_BUILD, alpha=ALPHA, seed=0)),
+    "hcnng": ("c2_hcnng_T30_L1000_m3.graph", "HCNNG 30 trees leaf1000 MST3",
+              lambda pgb, x: pgb.build_hcnng(x, trees=30, leaf=1000, mst_deg=3, seed=0)),
+    "nnd": ("c2_nnd_K40.graph", "PyNNDescent K40 alpha1.2",
+            lambda pgb, x: pgb.build_nndescent(x, K=40, init_trees=10, leaf=1000, alpha=1.2,
+                                               seed=0)),
+}
+HNSW_FILE = "c2_hnsw_M32_efc128.hnsw"
+
+
+def load_base(pgb):
     from parlayann_gpu_busqueda_b200 import synthetic as syn
-    d = data_dir()
-    base_p = os.path.join(d, "c2_base.i8bin")
-    graph_p = os.path.join(d, f"c2_vamana_R{R}_L{L_BUILD}_a{ALPHA}.graph")
+    base_p = os.path.join(data_dir(), "c2_base.i8bin")
+    if not os.path.exists(base_p):
+        base = syn.LAW_C2.sample(N_BASE, 0, 0)
+        pgb.write_vectors(base_p + ".tmp", base)
+        os.replace(base_p + ".tmp", base_p)
+    return pgb.read_vectors(base_p)
+
+
+def load_workload(pgb, rank, barrier, kind="vamana", nq=N_QUERIES):
+    """Base vectors, this rank's queries and a flat graph (built once, cached on disk)."""
+    from parlayann_gpu_busqueda_b200 import synthetic as syn
+    fname, _, build = GRAPHS[kind]
+    graph_p = os.path.join(data_dir(), fname)
     if rank == 0:
-        if not os.path.exists(base_p):
-            base = syn.LAW_C2.sample(N_BASE, 0, 0)
-            pgb.write_vectors(base_p + ".tmp", base)
-            os.replace(base_p + ".tmp", base_p)
+        base = load_base(pgb)
         if not os.path.exists(graph_p):
-            base = pgb.read_vectors(base_p)
             t = time.time()
-            g = pgb.build_vamana(base, R=R, L=L_BUILD, alpha=ALPHA, seed=0)
-            log(f"built Vamana 1M in {time.time() - t:.1f} s")
+            g = build(pgb, base)
+            log(f"built {kind} 1M in {time.time() - t:.1f} s")
             pgb.write_graph(graph_p + ".tmp", g)
             os.replace(graph_p + ".tmp", graph_p)
     barrier()
-    base = pgb.read_vectors(base_p)
+    base = load_base(pgb)
     graph = pgb.read_graph(graph_p)
-    queries = syn.LAW_C2.sample(N_QUERIES, 0, 1 + rank)
+    queries = syn.LAW_C2.sample(nq, 0, 1 + rank)
     return base, queries, graph
+
+
+def load_hnsw(pgb):
+    p = os.path.join(data_dir(), HNSW_FILE)
+    base = load_base(pgb)
+    if not os.path.exists(p):
+        t = time.time()
+        pgb.build_hnsw(base, p + ".tmp", M=32, ef_construction=128, ml=0.36, alpha=0.83, seed=0)
+        os.replace(p + ".tmp", p)
+        log(f"built HNSW 1M in {time.time() - t:.1f} s")
+    return base, pgb.read_hnsw(p)
 
 
 def ground_truth(base, queries, rank, device):
@@ -256,10 +285,19 @@ def main():
                          "warm-up then --steps launches of each kernel, nothing else")
     ap.add_argument("--profile-nq", type=int, default=8192)
     ap.add_argument("--profile-ls", type=int, default=40)
+    ap.add_argument("--workload", default="vamana",
+                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving"],
+                    help="vamana (default, the headline): plain vs batched at recall 0.90; "
+                         "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
+                         "mixed: 100k queries of uneven Ls and k in one launch; serving: "
+                         "Poisson bursts through the request loop")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.profile:
         run_profile(args, local)
+        return
+    if args.workload in ("hnsw", "mixed", "serving") and args.impl == "ours":
+        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -281,7 +319,7 @@ def main():
     pgb = ge.load_package()
     from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
     t0 = time.time()
-    base, queries, graph = load_workload(pgb, rank, barrier)
+    base, queries, graph = load_workload(pgb, rank, barrier, args.workload)
     gt_ids, gt_d = ground_truth(base, queries, rank, local)
     index = pgb.Index.flat(base, graph, device=local)
     log(f"rank {rank}: setup {time.time() - t0:.1f} s, index {index.info.device_bytes / 2**20:.0f} MiB")
@@ -437,7 +475,7 @@ def main():
             "data": "synthetic",
             "config": {
                 "workload": "1M int8 d=100 Gaussian mixture (1024 centres, sigma 10, 30% zeros), "
-                            "Vamana R64 L128 alpha1.2, 29316 queries per GPU, k=10",
+                            f"{GRAPHS[args.workload][1]}, 29316 queries per GPU, k=10",
                 "Ls": Ls, "recall_at_10": recall_at, "sweep_recall": sweep,
                 "parallelism": f"queries sharded, index replicated x{world}",
                 "l2": "flushed (512 MiB write) before every timed step; index 384 MB > L2",
@@ -467,6 +505,206 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _timed_events(torch, stream, fn, steps, warmup, flush=None):
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    out = []
+    for _ in range(steps):
+        if flush is not None:
+            flush.fill_(1)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        out.append(a.elapsed_time(b))
+    return out
+
+
+def run_hnsw(args, local):
+    """HNSW (M=32, efConstruction=128) on the 1M workload: QPS at recall@10 >= 0.90."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    from parlayann_gpu_busqueda_b200.synthetic import LAW_C2, LS_SWEEP
+    base, h = load_hnsw(pgb)
+    queries = LAW_C2.sample(N_QUERIES, 0, 1)
+    gt_ids, gt_d = ground_truth(base, queries, 0, local)
+    index = pgb.Index.hnsw(base, h, device=local)
+    q = torch.from_numpy(queries.view(np.uint8)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    sweep, Ls = [], None
+    for ls in LS_SWEEP:
+        s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=ls))
+        ids, _, _ = s.search_device(q, stream.cuda_stream)
+        torch.cuda.synchronize()
+        rec = pgb.recall(gt_ids, gt_d, ids.cpu().numpy().view(np.uint32), K)
+        sweep.append([ls, round(rec, 5)])
+        s.liberar()
+        if rec >= TARGET_RECALL and Ls is None:
+            Ls = ls
+        if Ls is not None and ls >= 2 * Ls:
+            break
+    Ls = Ls or LS_SWEEP[-1]
+    s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=Ls))
+    ids = torch.empty((N_QUERIES, K), dtype=torch.int32, device=dev)
+    d = torch.empty_like(ids)
+    st = torch.empty((N_QUERIES, 4), dtype=torch.int32, device=dev)
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+    t = _timed_events(torch, stream, lambda: s.lanzar(q, ids, d, st, stream.cuda_stream),
+                      args.steps, args.warmup, flush)
+    stn = st.cpu().numpy()
+    qps = N_QUERIES * len(t) / (sum(t) / 1e3)
+    G0 = (int(index.info.max_degree) + 31) // 32 * 32
+    bytes_launch = float(128 * stn[:, 0].astype(np.int64).sum() + 4 * G0 * stn[:, 1].astype(np.int64).sum())
+    peak, kind = measured_peaks()
+    achieved = bytes_launch / (sum(t) / len(t) / 1e3) / 1e9
+    print(json.dumps({
+        "metric": "QPS @ recall@10=0.90, HNSW search, 1 B200", "value": qps, "unit": "queries/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sum(t) / len(t), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": "1M int8 d=100 Gaussian mixture, HNSW M32 efc128, 29316 queries, k=10",
+                   "Ls": Ls, "recall_at_10": dict((a, b) for a, b in sweep)[Ls], "sweep_recall": sweep,
+                   "l2": "flushed before every timed step",
+                   "comps_per_query": float(stn[:, 0].mean()),
+                   "expansions_per_query": float(stn[:, 1].mean())},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "peak_source": kind,
+                     "kernel": "hnsw_kernel"},
+        "gpu_launches": args.steps}), flush=True)
+
+
+def run_mixed(args, local):
+    """100,000 queries with Ls log-uniform in [10, 500] and k in {10, 50, 100}: one batched
+    launch (CUDA graph) against the plain kernel launched once per distinct (Ls, k)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    nq = 100_000
+    base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana", nq)
+    rng = np.random.default_rng(0)
+    ls = np.rint(np.exp(rng.uniform(np.log(10), np.log(500), nq))).astype(np.uint32)
+    ks = rng.choice(np.array([10, 50, 100], np.uint32), nq)
+    max_k = 100
+    index = pgb.Index.flat(base, graph, device=local)
+    q = torch.from_numpy(queries.view(np.uint8)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    # the plain arm regroups queries, so the query-index exclusion is off in both arms
+    b = pgb.Batch(index, nq, max_beam=int(ls.max()), max_k=max_k, exclude_query_id=False)
+    b.plan(ls, ks)
+    ids, d, st = b.outputs(dev)
+    tuned = b.tune(q, ids, d, st)
+    b.capture(q, ids, d, st)
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+    steps = max(3, args.steps // 20)
+    tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, 2, flush)
+    # plain: the drop-in prepares one searcher per distinct (Ls, k) and launches it on
+    # that group's queries; preparing and releasing are outside the timed launches
+    groups = {}
+    for i in range(nq):
+        groups.setdefault((int(ls[i]), int(ks[i])), []).append(i)
+    got = ids.cpu().numpy().view(np.uint32)
+    same, t_plain_ms = True, 0.0
+    for (L, k), idx in groups.items():
+        idx = np.array(idx)
+        qi = torch.from_numpy(queries[idx].view(np.uint8)).to(dev)
+        s = pgb.Searcher(index, len(idx), pgb.QueryParams(k=k, beam_size=L,
+                                                          exclude_query_id=False))
+        oi = torch.empty((len(idx), k), dtype=torch.int32, device=dev)
+        od = torch.empty_like(oi)
+        t_plain_ms += sum(_timed_events(torch, stream, lambda: s.lanzar(qi, oi, od, None, sp),
+                                        1, 1))
+        same = same and np.array_equal(oi.cpu().numpy().view(np.uint32), got[idx, :k])
+        s.liberar()
+    qb = nq * len(tb) / (sum(tb) / 1e3)
+    qp = nq / (t_plain_ms / 1e3)
+    plain = list(groups)
+    print(json.dumps({
+        "metric": "QPS, 100k queries of uneven Ls and k, batched (one launch) vs plain", "value": qb,
+        "unit": "queries/s", "n_gpus": 1, "steps": steps, "warmup": 2,
+        "ms_per_step": sum(tb) / len(tb), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": "1M int8 d=100 Vamana R64, 100000 queries, Ls log-uniform [10,500], "
+                               "k in {10,50,100}", "batched_qps": qb, "plain_qps": qp,
+                   "plain_launches_per_step": len(plain), "batched_over_plain": qb / qp,
+                   "plain_timing": "sum of per-group launch times (events), L2 warm",
+                   "identical_neighbours": bool(same), "batched_config": tuned,
+                   "l2": "flushed before every timed step"},
+        "gpu_launches": steps + len(plain)}), flush=True)
+
+
+def run_serving(args, local):
+    """Poisson arrivals of single queries and bursts (1-256) at offered rates from 10k to
+    2M QPS through the request loop; per-request Ls in {20,50,100,300}, k in {10,100}."""
+    import torch
+    torch.cuda.set_device(local)
+    pgb = ge.load_package()
+    base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana")
+    gt_ids, gt_d = ground_truth(base, queries, 0, local)
+    index = pgb.Index.flat(base, graph, device=local)
+    rng = np.random.default_rng(1)
+    rates = [int(r) for r in os.environ.get("PGB_SERVE_RATES",
+                                            "10000,100000,500000,1000000,2000000").split(",")]
+    seconds = float(os.environ.get("PGB_SERVE_SECONDS", "1.5"))
+    rows = []
+    for rate in rates:
+        srv = pgb.Server(index, max_beam=300, max_k=100, max_batch=2048, max_inflight=4)
+        # arrival events: half single queries, half bursts uniform in 2..256
+        mean_burst = 0.5 * 1 + 0.5 * 129
+        n_events = max(1, int(rate * seconds / mean_burst))
+        gaps = rng.exponential(mean_burst / rate, n_events)
+        sizes = np.where(rng.random(n_events) < 0.5, 1, rng.integers(2, 257, n_events))
+        t_evt = np.cumsum(gaps)
+        outstanding, issued, done_q, recalls = [], 0, 0, []
+        t0 = time.perf_counter()
+        ev = 0
+        while ev < n_events or outstanding:
+            now = time.perf_counter() - t0
+            while ev < n_events and t_evt[ev] <= now:
+                m = int(sizes[ev])
+                sel = rng.integers(0, N_QUERIES, m)
+                L = rng.choice(np.array([20, 50, 100, 300], np.uint32), m)
+                k = rng.choice(np.array([10, 100], np.uint32), m)
+                t = srv.submit_many(queries[sel], L, k)
+                outstanding.append((t, sel[:len(t)]))
+                issued += len(t)
+                ev += 1
+            if outstanding:
+                tk = np.concatenate([o[0] for o in outstanding])
+                qs = np.concatenate([o[1] for o in outstanding])
+                done, oi, _, _ = srv.poll_many(tk)
+                if done.any():
+                    rec = pgb.recall(gt_ids[qs[done]], gt_d[qs[done]], oi[done][:, :K], K)
+                    recalls.append((rec, int(done.sum())))
+                    done_q += int(done.sum())
+                    outstanding = [(tk[~done], qs[~done])] if (~done).any() else []
+            if now > 20 * seconds:
+                break
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        rec = sum(r * n for r, n in recalls) / max(1, sum(n for _, n in recalls))
+        rows.append({"offered_qps": rate, "sustained_qps": done_q / wall, "p50_us": st["p50_us"],
+                     "p99_us": st["p99_us"], "rejected": st["rejected"], "launches": st["launches"],
+                     "mean_batch": st["mean_batch"], "recall_at_10": rec})
+        log(rows[-1])
+    best = max(rows, key=lambda r: r["sustained_qps"])
+    print(json.dumps({
+        "metric": "serving p50/p99 latency and sustained QPS, Poisson bursts, 1 B200",
+        "value": best["sustained_qps"], "unit": "queries/s", "n_gpus": 1, "steps": len(rows),
+        "warmup": 0, "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": "1M int8 d=100 Vamana R64, per-request Ls in {20,50,100,300}, k in "
+                               "{10,100}, bursts of 1-256", "rates": rows},
+        "gpu_launches": int(sum(r["launches"] for r in rows))}), flush=True)
 
 
 if __name__ == "__main__":

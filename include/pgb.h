@@ -239,6 +239,18 @@ pgb_status pgb_server_submit(pgb_server* s, const void* query, uint32_t beam_siz
  * success copies k ids / dists (and stats, may be NULL) and releases the ticket. */
 pgb_status pgb_server_poll(pgb_server* s, uint64_t ticket, uint32_t timeout_us, uint32_t* ids,
                            int32_t* dists, pgb_query_stats* stats);
+/* A burst: n queries query_stride bytes apart with their own beam sizes and k. Admits the
+ * longest prefix that fits; *admitted tells how many (tickets[0..admitted)); PGB_OK even
+ * when only part of the burst fit, PGB_ERR_BUSY when none did. */
+pgb_status pgb_server_submit_many(pgb_server* s, const void* queries, uint32_t n,
+                                  uint32_t query_stride, const uint32_t* beam_sizes,
+                                  const uint32_t* ks, uint64_t* tickets, uint32_t* admitted);
+/* Non-blocking sweep over n tickets: done[i] = 1 and row i of ids / dists (stride max_k)
+ * and stats[i] (may be NULL) filled for every finished request, whose ticket is released;
+ * done[i] = 0 otherwise. *n_done counts the finished ones. Unknown tickets are skipped. */
+pgb_status pgb_server_poll_many(pgb_server* s, const uint64_t* tickets, uint32_t n,
+                                uint32_t* ids, int32_t* dists, pgb_query_stats* stats,
+                                uint8_t* done, uint32_t* n_done);
 pgb_status pgb_server_get_stats(pgb_server* s, pgb_server_stats* out);
 /* completes the requests in flight, then frees everything */
 pgb_status pgb_server_destroy(pgb_server* s);

@@ -144,4 +144,6 @@ _sig("pgb_server_create", C.c_int, vp, C.POINTER(ServerOptions), C.POINTER(vp))
 _sig("pgb_server_submit", C.c_int, vp, vp, u32, u32, C.POINTER(C.c_uint64))
 _sig("pgb_server_poll", C.c_int, vp, C.c_uint64, u32, vp, vp, vp)
 _sig("pgb_server_get_stats", C.c_int, vp, C.POINTER(ServerStats))
+_sig("pgb_server_submit_many", C.c_int, vp, vp, u32, u32, vp, vp, vp, C.POINTER(C.c_uint32))
+_sig("pgb_server_poll_many", C.c_int, vp, vp, u32, vp, vp, vp, vp, C.POINTER(C.c_uint32))
 _sig("pgb_server_destroy", C.c_int, vp)

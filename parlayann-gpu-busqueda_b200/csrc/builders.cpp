@@ -470,8 +470,9 @@ int build_nndescent(const HostVectors& V, uint32_t K, uint32_t init_trees, uint3
 
 // ---------------------------------------------------------------------------
 // HNSW with batch insertion. Levels l = floor(-ln(U) * ml); level-0 rows hold 2M
-// neighbours, upper rows M; neighbour selection by the HNSW heuristic with the
-// alpha relaxation (keep c unless alpha * d(o, c) < d(p, c) for a kept o).
+// neighbours, upper rows M; neighbour selection by the HNSW heuristic with an alpha
+// relaxation (keep c unless d(o, c) < alpha * d(p, c) for a kept o; alpha = 1 is the
+// plain heuristic, alpha < 1 keeps more neighbours).
 
 static void hnsw_select(const HostVectors& V, uint32_t p, std::vector<DistId>& cand,
                         float alpha, uint32_t cap, std::vector<uint32_t>& out) {
@@ -485,7 +486,7 @@ static void hnsw_select(const HostVectors& V, uint32_t p, std::vector<DistId>& c
         if (c.id == p) continue;
         bool keep = true;
         for (uint32_t o : out)
-            if (alpha * (float)V.dist(o, c.id) < (float)c.d) {
+            if ((float)V.dist(o, c.id) < alpha * (float)c.d) {
                 keep = false;
                 break;
             }

@@ -433,6 +433,76 @@ pgb_status pgb_server_poll(pgb_server* S, uint64_t ticket, uint32_t timeout_us, 
     return PGB_OK;
 }
 
+pgb_status pgb_server_submit_many(pgb_server* S, const void* queries, uint32_t n,
+                                  uint32_t query_stride, const uint32_t* beam_sizes,
+                                  const uint32_t* ks, uint64_t* tickets, uint32_t* admitted) {
+    if (!S || !queries || !beam_sizes || !ks || !tickets || !admitted)
+        return fail(PGB_ERR_BAD_ARG, "null argument");
+    *admitted = 0;
+    if (query_stride < S->index->dim) return fail(PGB_ERR_BAD_ARG, "query_stride below dim");
+    for (uint32_t i = 0; i < n; i++) {
+        if (beam_sizes[i] == 0 || beam_sizes[i] > S->opt.max_beam)
+            return fail(PGB_ERR_BAD_ARG, "beam size outside 1..max_beam");
+        if (ks[i] == 0 || ks[i] > S->opt.max_k) return fail(PGB_ERR_BAD_ARG, "k outside 1..max_k");
+    }
+    uint32_t got = 0;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->failed != PGB_OK) return fail(S->failed, S->fail_msg);
+        if (S->stop) return fail(PGB_ERR_BAD_ARG, "server is shutting down");
+        const auto now = Clock::now();
+        const uint8_t* q = static_cast<const uint8_t*>(queries);
+        for (; got < n && !S->free_slots.empty(); got++) {
+            const uint32_t slot = S->free_slots.back();
+            S->free_slots.pop_back();
+            Slot& sl = S->pool[slot];
+            memcpy(sl.query.data(), q + (size_t)got * query_stride, S->index->dim);
+            sl.Ls = beam_sizes[got];
+            sl.k = ks[got];
+            sl.done = false;
+            sl.ticket = S->next_ticket++;
+            sl.t_submit = now;
+            S->by_ticket[sl.ticket] = slot;
+            S->pending.push_back(slot);
+            tickets[got] = sl.ticket;
+        }
+        S->submitted += got;
+        S->rejected += n - got;
+    }
+    *admitted = got;
+    if (got) S->cv_work.notify_one();
+    if (got == 0 && n > 0) return fail(PGB_ERR_BUSY, "request pool full");
+    return PGB_OK;
+}
+
+pgb_status pgb_server_poll_many(pgb_server* S, const uint64_t* tickets, uint32_t n,
+                                uint32_t* ids, int32_t* dists, pgb_query_stats* stats,
+                                uint8_t* done, uint32_t* n_done) {
+    if (!S || !tickets || !ids || !dists || !done || !n_done)
+        return fail(PGB_ERR_BAD_ARG, "null argument");
+    const size_t mk = S->opt.max_k;
+    uint32_t cnt = 0;
+    std::lock_guard<std::mutex> lk(S->mu);
+    for (uint32_t i = 0; i < n; i++) {
+        done[i] = 0;
+        auto it = S->by_ticket.find(tickets[i]);
+        if (it == S->by_ticket.end()) continue;
+        const uint32_t slot = it->second;
+        Slot& sl = S->pool[slot];
+        if (!sl.done) continue;
+        std::copy(sl.ids.begin(), sl.ids.begin() + sl.k, ids + i * mk);
+        std::copy(sl.dists.begin(), sl.dists.begin() + sl.k, dists + i * mk);
+        if (stats) stats[i] = sl.stats;
+        S->by_ticket.erase(it);
+        S->free_slots.push_back(slot);
+        done[i] = 1;
+        cnt++;
+    }
+    *n_done = cnt;
+    if (S->failed != PGB_OK && cnt == 0) return fail(S->failed, S->fail_msg);
+    return PGB_OK;
+}
+
 pgb_status pgb_server_get_stats(pgb_server* S, pgb_server_stats* out) {
     if (!S || !out) return fail(PGB_ERR_BAD_ARG, "null argument");
     std::vector<float> lat;

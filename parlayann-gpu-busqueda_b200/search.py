@@ -354,6 +354,33 @@ class Server:
         N.check(st)
         return ids, dists, stats
 
+    def submit_many(self, queries: np.ndarray, beam_sizes, ks):
+        """Burst submission; returns the tickets of the admitted prefix (may be empty)."""
+        q = np.ascontiguousarray(queries)
+        ls = np.ascontiguousarray(beam_sizes, dtype=np.uint32)
+        kk = np.ascontiguousarray(ks, dtype=np.uint32)
+        t = np.empty(len(q), np.uint64)
+        got = C.c_uint32()
+        st = N.lib.pgb_server_submit_many(self._h, _ptr(q), len(q), q.shape[1], _ptr(ls),
+                                          _ptr(kk), _ptr(t), C.byref(got))
+        if st == self.BUSY:
+            return t[:0]
+        N.check(st)
+        return t[:got.value]
+
+    def poll_many(self, tickets: np.ndarray):
+        """Non-blocking: (done mask, ids [n, max_k], dists [n, max_k], stats [n, 4])."""
+        t = np.ascontiguousarray(tickets, dtype=np.uint64)
+        n = len(t)
+        ids = np.empty((n, self.max_k), np.uint32)
+        dists = np.empty((n, self.max_k), np.int32)
+        stats = np.empty((n, 4), np.int32)
+        done = np.zeros(n, np.uint8)
+        cnt = C.c_uint32()
+        N.check(N.lib.pgb_server_poll_many(self._h, _ptr(t), n, _ptr(ids), _ptr(dists),
+                                           _ptr(stats), _ptr(done), C.byref(cnt)))
+        return done.astype(bool), ids, dists, stats
+
     def stats(self) -> dict:
         s = N.ServerStats()
         N.check(N.lib.pgb_server_get_stats(self._h, C.byref(s)))
