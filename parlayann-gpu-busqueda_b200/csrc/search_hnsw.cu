@@ -38,9 +38,13 @@ __host__ __device__ inline uint32_t hnsw_cap_inw(uint32_t Ls) {
 
 struct HnswLayout {
     uint32_t wcap, gs, filter_words;
-    uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_filter,
-        bytes;
+    uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_ibits,
+        off_filter, bytes;
 };
+
+// "maybe in is_inw" bitmap per warp: a clear bit proves absence, so most membership
+// checks never touch the global table
+constexpr uint32_t kInwBits = 4096;
 
 __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t gs,
                                                        uint32_t filter_words) {
@@ -67,6 +71,8 @@ __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t g
     o = round16(o + gs);
     L.off_eps = o;
     o += 4u * PGB_MAX_HNSW_ENTRIES;
+    L.off_ibits = o;
+    o += kInwBits / 8u;
     L.off_filter = o;
     o += 4u * filter_words;
     L.bytes = round16(o);
@@ -96,6 +102,10 @@ struct HnswArgs {
     unsigned long long* gfilter;
     uint64_t epoch_base;
 };
+
+__device__ __forceinline__ uint32_t inw_bit(uint32_t id) {
+    return (uint32_t)(hash64_2(id) >> 48) & (kInwBits - 1u);
+}
 
 __device__ __forceinline__ unsigned long long tag(uint32_t epoch, uint32_t id) {
     return ((unsigned long long)epoch << 32) | id;
@@ -132,7 +142,7 @@ __device__ void inw_insert(unsigned long long* tab, uint32_t mask, uint32_t epoc
 }
 
 template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
+__global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -151,6 +161,7 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
     int32_t* pos = reinterpret_cast<int32_t*>(wmem + L.off_pos);
     uint8_t* fl = wmem + L.off_fl;
     uint32_t* eps = reinterpret_cast<uint32_t*>(wmem + L.off_eps);
+    uint32_t* ibits = reinterpret_cast<uint32_t*>(wmem + L.off_ibits);
     uint32_t* sfilter = reinterpret_cast<uint32_t*>(wmem + L.off_filter);
     unsigned long long* inw = A.inw + (size_t)gw * A.cap_inw;
     unsigned long long* gfil = SFILT ? nullptr : A.gfilter + (size_t)gw * A.filter_slots;
@@ -182,8 +193,10 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
                 (uint32_t)(A.epoch_base + (uint64_t)q * layers + (A.top - (uint32_t)layer) + 1u);
             if (SFILT) {
                 for (uint32_t i = lane; i <= fmask; i += 32) sfilter[i] = kEmptyId;
-                __syncwarp();
             }
+            // this layer's is_inw is empty: clear its bitmap (32 lanes x 16 bytes)
+            reinterpret_cast<uint4*>(ibits)[lane] = make_uint4(0, 0, 0, 0);
+            __syncwarp();
             // ---- entry points: distances, then the sequential inserts on lane 0 ----
             for (int e = lane; e < neps; e += 32) pend[e] = eps[e];
             __syncwarp();
@@ -198,6 +211,8 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
                     if (SFILT) sfilter[s] = pe;
                     else gfil[s] = tag(epoch, pe);
                     inw_insert(inw, inw_mask, epoch, pe);
+                    const uint32_t b = inw_bit(pe);
+                    ibits[b >> 5] |= 1u << (b & 31u);
                     // cand: by distance, equal distance rejected
                     const uint64_t key = pack_key(d, pe);
                     int pos = lower_bound_key(ckey, nC, pack_key(d, 0));
@@ -323,7 +338,12 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
                             first = false;
                             break;
                         }
-                    fl[j] = (first && !inw_contains(inw, inw_mask, epoch, pv)) ? 1 : 0;
+                    bool in_w = false;
+                    if (first) {
+                        const uint32_t b = inw_bit(pv);
+                        if ((ibits[b >> 5] >> (b & 31u)) & 1u) in_w = inw_contains(inw, inw_mask, epoch, pv);
+                    }
+                    fl[j] = (first && !in_w) ? 1 : 0;
                 }
                 __syncwarp();
                 // ---- acceptance: fewer than m elements of W + earlier eligible at <= d
@@ -348,7 +368,12 @@ __global__ void __launch_bounds__(256) hnsw_kernel(HnswArgs A) {
                 __syncwarp();
                 if (na > 0) {
                     inserted += (uint32_t)na;
-                    for (int j = lane; j < na; j += 32) inw_insert(inw, inw_mask, epoch, key_id(akey[j]));
+                    for (int j = lane; j < na; j += 32) {
+                        const uint32_t id = key_id(akey[j]);
+                        inw_insert(inw, inw_mask, epoch, id);
+                        const uint32_t b = inw_bit(id);
+                        atomicOr(&ibits[b >> 5], 1u << (b & 31u));
+                    }
                     // ---- cand update (accepted keys still in arrival order) ---------------
                     const int nC0 = nC;
                     if (nC0 <= ef) {
@@ -508,7 +533,9 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     H.bits0 = hnsw_bits0(Ls);
     H.cap_inw = hnsw_cap_inw(Ls);
     const uint32_t fwords = 1u << H.bits0;
-    H.sfilt = 4ull * fwords <= 16384;
+    // shared-memory filter only while small (Ls <= 64): a 16 KB filter would cap the
+    // kernel at 8 resident warps per SM; larger ones use the epoch-tagged global table
+    H.sfilt = 4ull * fwords <= 4096;
     H.filter_slots = H.sfilt ? 0u : fwords;
     H.wcap = ((std::max<uint32_t>(Ls, PGB_MAX_HNSW_ENTRIES) + 8u) + 7u) & ~7u;
     const HnswLayout L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? fwords : 0u);
@@ -528,6 +555,9 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     // per-kernel attribute shared by all searchers: the device maximum, never shrunk
     if ((s = hnsw_cuda(cudaFuncSetAttribute(H.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)prop.sharedMemPerBlockOptin),
+                       "cudaFuncSetAttribute")) != PGB_OK ||
+        (s = hnsw_cuda(cudaFuncSetAttribute(H.kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            (int)cudaSharedmemCarveoutMaxShared),
                        "cudaFuncSetAttribute")) != PGB_OK)
         return s;
     int bps = 0;
