@@ -93,7 +93,7 @@ struct FlatLayout {
 
 // "maybe visited" bitmap per warp: a node's bit is set when it is expanded, so a
 // candidate whose bit is clear has never been expanded and needs no table lookup
-constexpr uint32_t kVisitedBits = 1024;
+constexpr uint32_t kVisitedBits = 1024;  // visited_bit() yields 10 bits
 
 __host__ __device__ inline uint32_t round16(uint32_t x) { return (x + 15u) & ~15u; }
 
@@ -155,8 +155,14 @@ struct FlatArgs {
 };
 
 // ---- exact visited multiset (keys only; duplicates occupy several slots) ----------
-__device__ __forceinline__ uint32_t visited_home(uint32_t id, uint32_t mask) {
-    return (uint32_t)(hash64_2(id) >> 32) & mask;  // reference busqueda.cu:58-60
+// Slot positions in this table and in the bitmap are private (only the counts matter),
+// so they use 32-bit multiplicative hashes (Knuth's golden-ratio constant for the home
+// slot's top bits, a second odd constant for the bitmap bit) instead of hash64_2.
+__device__ __forceinline__ uint32_t visited_home(uint32_t id, uint32_t shift) {
+    return (id * 0x9E3779B1u) >> shift;
+}
+__device__ __forceinline__ uint32_t visited_bit(uint32_t id) {
+    return (id * 0x85EBCA6Bu) >> (32 - 10);  // 1,024-bit bitmap
 }
 
 // continues an insert whose first 32 probe slots were all taken
@@ -373,6 +379,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     const uint32_t fmask = (1u << flat_filter_bits(Ls)) - 1u;
     const uint32_t vcap = flat_visited_cap(Ls);
     const uint32_t vmask = vcap - 1u;
+    const uint32_t vshift = 32u - (uint32_t)ceil_log2_u64(vcap);
     const int max_visits = (int)(vcap / 2u);
     const int64_t limit = A.limit;
     const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
@@ -434,12 +441,11 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         // visited insert of cur, in two halves: the 32 probe slots are read now and the
         // slot is claimed at the end of the iteration (only this warp writes the table);
         // lookups in between add the pending copy themselves
-        const uint64_t hcur = hash64_2(cur);
-        const uint32_t vhome = (uint32_t)(hcur >> 32) & vmask;
+        const uint32_t vhome = visited_home(cur, vshift);
         const uint32_t vslot = (vhome + (uint32_t)lane) & vmask;
         const uint32_t vprobe = vtab[vslot];
         if (lane == 0) {
-            const uint32_t b = (uint32_t)(hcur >> 48) & (kVisitedBits - 1u);
+            const uint32_t b = visited_bit(cur);
             vbits[b >> 5] |= 1u << (b & 31u);
         }
         nvis++;
@@ -543,12 +549,13 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         // is requested as soon as that is known, before the frontier is shifted
         uint64_t best = (u2 >= 0 && u2 < fsize) ? fkey[u2] : kEmptyKey;
 
-        int unew = u, minpos = INT_MAX;
+        int unew = u;
         int ne = 0;
         if (nc > 0) {
             sort_keys<CH>(ckey, nc, lane);
             PGB_PROF_ADD(SEC_SORT, tp);
             // ---- multiset set_union: copy `rep` of a key enters iff rep >= copies in F
+            bool found = false;  // best unvisited entering key seen (keys ascend)
             for (int base = 0; base < nc; base += 32) {
                 const int i = base + lane;
                 bool enter = false;
@@ -565,11 +572,10 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                     enter = rep >= cf;
                     if (enter) {
                         const uint32_t id = key_id(key);
-                        const uint64_t hh = hash64_2(id);
-                        const uint32_t b = (uint32_t)(hh >> 48) & (kVisitedBits - 1u);
+                        const uint32_t b = visited_bit(id);
                         int cnt = 0;
                         if ((vbits[b >> 5] >> (b & 31u)) & 1u)
-                            cnt = visited_count(vtab, vmask, id, (uint32_t)(hh >> 32) & vmask) +
+                            cnt = visited_count(vtab, vmask, id, visited_home(id, vshift)) +
                                   (id == cur ? 1 : 0);
                         vis = (uint8_t)(rep < cnt);
                     }
@@ -578,8 +584,13 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 // new copies follow the frontier copies of an equal key
                 const int pos = hi + ne + __popc(m & lt);
                 const bool keep = enter && pos < (int)Ls;
-                if (keep && !vis) best = key < best ? key : best;
                 const uint32_t mk = __ballot_sync(kFull, keep);
+                const uint32_t mnv = __ballot_sync(kFull, keep && !vis);
+                if (mnv && !found) {
+                    const uint64_t k0 = __shfl_sync(kFull, key, __ffs(mnv) - 1);
+                    best = k0 < best ? k0 : best;
+                    found = true;
+                }
                 if (keep) {
                     const int jk = ne + __popc(mk & lt);
                     ekey[jk] = key;
@@ -590,11 +601,6 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
                 if (mk != m) break;  // later keys land at or past Ls
             }
             __syncwarp();
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const uint64_t o = __shfl_xor_sync(kFull, best, off);
-                best = o < best ? o : best;
-            }
         }
         pred = (best != kEmptyKey) ? key_id(best) : kEmptyId;
         if (pred != kEmptyId) {
@@ -606,65 +612,73 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
             }
         }
         PGB_PROF_ADD(SEC_UNION, tp);
-        {
-            if (ne > 0) {
-                // the expanded entry's new position, then shift the frontier tail
-                unew = u + lower_bound_key(ekey, ne, cur_key);
-                const int first = epos[0];
-                for (int top = fsize - 1; top >= first; top -= 32) {
-                    const int i = top - lane;
-                    const bool act = i >= first;
-                    uint64_t key = 0;
-                    uint8_t vis = 0;
-                    int np2 = 0;
-                    if (act) {
-                        key = fkey[i];
-                        vis = fvis[i];
-                        np2 = i + lower_bound_key(ekey, ne, key);
-                    }
-                    __syncwarp();
-                    if (act && np2 < (int)Ls) {
-                        fkey[np2] = key;
-                        fvis[np2] = vis;
-                    }
-                    __syncwarp();
-                }
-                for (int j = lane; j < ne; j += 32) {
-                    fkey[epos[j]] = ekey[j];
-                    fvis[epos[j]] = evis[j];
-                    if (!evis[j]) minpos = min(minpos, epos[j]);
+
+        int from;
+        if (ne > 0) {
+            // the expanded entry's new position, then shift the frontier tail
+            unew = u + lower_bound_key(ekey, ne, cur_key);
+            const int first = epos[0];
+            for (int top = fsize - 1; top >= first; top -= 32) {
+                const int i = top - lane;
+                const bool act = i >= first;
+                uint64_t key = 0;
+                uint8_t vis = 0;
+                int np2 = 0;
+                if (act) {
+                    key = fkey[i];
+                    vis = fvis[i];
+                    np2 = i + lower_bound_key(ekey, ne, key);
                 }
                 __syncwarp();
-                fsize = min((int)Ls, fsize + ne);
+                if (act && np2 < (int)Ls) {
+                    fkey[np2] = key;
+                    fvis[np2] = vis;
+                }
+                __syncwarp();
             }
-        }
-        PGB_PROF_ADD(SEC_SHIFT, tp);
+            int minpos = INT_MAX;
+            for (int j = lane; j < ne; j += 32) {
+                fkey[epos[j]] = ekey[j];
+                fvis[epos[j]] = evis[j];
+                if (!evis[j]) minpos = min(minpos, epos[j]);
+            }
+            __syncwarp();
+            fsize = min((int)Ls, fsize + ne);
+            PGB_PROF_ADD(SEC_SHIFT, tp);
 
-        // ---- cut --------------------------------------------------------------------
-        if (fsize > (int)k) {
-            const float thr = (float)(A.cut * (double)key_dist(fkey[k]));
-            int newsize = fsize;
-            for (int base = 0; base < fsize; base += 32) {
-                const int i = base + lane;
-                bool after = false;
-                if (i < fsize) {
-                    const uint64_t e = fkey[i];
-                    const float de = (float)key_dist(e);
-                    after = thr < de || (thr == de && 0u < key_id(e));
+            // ---- cut (only a changed frontier can need one) ---------------------------
+            if (fsize > (int)k) {
+                const float thr = (float)(A.cut * (double)key_dist(fkey[k]));
+                // "after the threshold" is monotone along F: when the last entry is not
+                // after it, nothing is cut (the common case once the beam has converged)
+                const uint64_t last = fkey[fsize - 1];
+                const float dl = (float)key_dist(last);
+                const bool any_cut = thr < dl || (thr == dl && 0u < key_id(last));
+                int newsize = fsize;
+                for (int base = 0; any_cut && base < fsize; base += 32) {
+                    const int i = base + lane;
+                    bool after = false;
+                    if (i < fsize) {
+                        const uint64_t e = fkey[i];
+                        const float de = (float)key_dist(e);
+                        after = thr < de || (thr == de && 0u < key_id(e));
+                    }
+                    const uint32_t m = __ballot_sync(kFull, after);
+                    if (m) {
+                        newsize = base + __ffs(m) - 1;
+                        break;
+                    }
                 }
-                const uint32_t m = __ballot_sync(kFull, after);
-                if (m) {
-                    newsize = base + __ffs(m) - 1;
-                    break;
-                }
+                fsize = newsize;
             }
-            fsize = newsize;
+            minpos = (int)__reduce_min_sync(kFull, (unsigned)minpos);
+            from = min(unew, minpos);
+        } else {
+            // unchanged frontier (already cut): the next unvisited entry is the second one
+            from = (u2 >= 0) ? u2 : u + 1;
         }
 
         // ---- next unvisited ---------------------------------------------------------
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) minpos = min(minpos, __shfl_xor_sync(kFull, minpos, off));
-        const int from = min(unew, minpos);
         u = -1;
         u2 = -1;
         for (int base = from; base < fsize; base += 32) {
