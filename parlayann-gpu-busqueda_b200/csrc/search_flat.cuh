@@ -288,11 +288,14 @@ __device__ __forceinline__ void sort_keys(uint64_t* keys, int nc, int lane) {
     }
 }
 
-// ---- distances of pending rows: 4 lanes per 128-byte row, 16 rows in flight ---------
+// ---- distances of pending rows: 4 lanes per 128-byte row, 8*SLOTS rows in flight ---
 // Lane c of a row reads its 16-byte words c and c+4, so each load instruction covers two
 // whole 32-byte sectors of 8 rows. q4: the query row (128 bytes, shared memory).
 // norm_in_row: the row's squared norm sits in bytes 124..127 (word 7, held by lane 3).
-template <bool Signed>
+#ifndef PGB_DIST_SLOTS
+#define PGB_DIST_SLOTS 2
+#endif
+template <bool Signed, int SLOTS = PGB_DIST_SLOTS>
 __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
                                               const uint32_t* ids, int32_t* out, int np,
                                               const int4* q4, const int32_t qq, uint32_t dim,
@@ -302,10 +305,10 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
     // bytes past dim are zero in every row; lane 3 also loads word 7 when it holds the norm
     const bool need_a = (uint32_t)(c * 16) < dim;
     const bool need_b = (uint32_t)((c + 4) * 16) < dim || (norm_in_row && c == 3);
-    for (int base = 0; base < np; base += 16) {
-        int4 va[2], vb[2];
+    for (int base = 0; base < np; base += 8 * SLOTS) {
+        int4 va[SLOTS], vb[SLOTS];
 #pragma unroll
-        for (int r = 0; r < 2; r++) {
+        for (int r = 0; r < SLOTS; r++) {
             const int i = base + r * 8 + grp;
             va[r] = make_int4(0, 0, 0, 0);
             vb[r] = make_int4(0, 0, 0, 0);
@@ -315,24 +318,24 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
                 if (need_b) vb[r] = ldg16(row + 64);
             }
         }
-        int32_t t[2];
+        int32_t t[SLOTS];
         if (norm_in_row) {
 #pragma unroll
-            for (int r = 0; r < 2; r++)
+            for (int r = 0; r < SLOTS; r++)
                 t[r] = (c == 3 ? vb[r].w : 0) -
                        2 * (partial_dot<Signed>(va[r], qa) + partial_dot<Signed>(vb[r], qb));
         } else {
 #pragma unroll
-            for (int r = 0; r < 2; r++)
+            for (int r = 0; r < SLOTS; r++)
                 t[r] = partial_l2<Signed>(va[r], qa) + partial_l2<Signed>(vb[r], qb);
         }
 #pragma unroll
         for (int off = 2; off > 0; off >>= 1)
 #pragma unroll
-            for (int r = 0; r < 2; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 4);
+            for (int r = 0; r < SLOTS; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 4);
         if (c == 0) {
 #pragma unroll
-            for (int r = 0; r < 2; r++) {
+            for (int r = 0; r < SLOTS; r++) {
                 const int i = base + r * 8 + grp;
                 if (i < np) out[i] = qq + t[r];
             }
