@@ -12,6 +12,12 @@
 #include "search_flat.cuh"
 #include "search_plan.h"
 
+// resident 128-thread blocks per SM the flat kernels are compiled for (registers per
+// thread = 65536 / (128 * this)): 9 -> 56 registers, 36 warps per SM
+#ifndef PGB_MIN_BLOCKS
+#define PGB_MIN_BLOCKS 9
+#endif
+
 namespace pgb {
 
 #ifdef PGB_SECTION_PROFILE
@@ -36,7 +42,7 @@ __device__ unsigned long long g_section_cycles[NUM_SECTIONS];
 #endif
 
 template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(128, 9) flat_plain_kernel(FlatArgs A) {
+__global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_plain_kernel(FlatArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -53,7 +59,7 @@ __global__ void __launch_bounds__(128, 9) flat_plain_kernel(FlatArgs A) {
 }
 
 template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(128, 9) flat_batched_kernel(FlatArgs A) {
+__global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_batched_kernel(FlatArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
