@@ -154,6 +154,29 @@ pgb_status pgb_searcher_search_host(pgb_searcher* s, const void* queries, uint32
 /* liberar */
 pgb_status pgb_searcher_destroy(pgb_searcher* s);
 
+/* ---- plain search without device allocation (no counterpart in the reference) ------
+ * For callers that may not allocate device memory at query time: cudaMalloc and cudaFree
+ * can synchronise the whole device (stalling every other stream of a serving process),
+ * and a host framework's caching allocator may already hold the device's free memory.
+ * The same plain kernel and results as pgb_searcher_search with these params, but with
+ * its per-warp visited tables in one fixed array inside the library
+ * (PGB_NOALLOC_SCRATCH_BYTES on every device that loads the library, held until exit)
+ * instead of a searcher's scratch; the lossy filter stays in shared memory, which caps
+ * the beam at PGB_NOALLOC_MAX_BEAM (larger beams fail with PGB_ERR_BAD_ARG). Flat-graph
+ * indexes only. Wide beams run on fewer warps, as many as the array holds tables for.
+ * The first call on each device (made with that device current) looks up the array's
+ * device address; make that first call before any stream capture. Every call on a device
+ * shares the one array: calls whose kernels overlap on the GPU (other streams, other host
+ * threads) race on it and return wrong neighbours, so order them on one stream or
+ * synchronise between them. Nothing in the array has to start at zero: each query clears
+ * its own table before use. Arguments and outputs as pgb_searcher_search; any nq. */
+#define PGB_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define PGB_NOALLOC_MAX_BEAM 128u
+pgb_status pgb_search_flat_noalloc(const pgb_index* index, const pgb_query_params* params,
+                                   const void* queries, uint32_t nq, uint32_t query_stride,
+                                   uint32_t* ids, int32_t* dists, pgb_query_stats* stats,
+                                   void* stream);
+
 /* ---- batched persistent form (no counterpart in the reference) -----------------------
  * One persistent launch serves queries of different beam sizes and k: warps pull the next
  * query from a device counter over a longest-beam-first order, so a long beam never holds
