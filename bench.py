@@ -81,7 +81,6 @@ def load_base(pgb):
 
 def load_workload(pgb, rank, barrier, kind="vamana", nq=N_QUERIES):
     """Base vectors, this rank's queries and a flat graph (built once, cached on disk)."""
-    from parlayann_gpu_busqueda_b200 import synthetic as syn
     fname, _, build = GRAPHS[kind]
     graph_p = os.path.join(data_dir(), fname)
     if rank == 0:
@@ -95,8 +94,30 @@ def load_workload(pgb, rank, barrier, kind="vamana", nq=N_QUERIES):
     barrier()
     base = load_base(pgb)
     graph = pgb.read_graph(graph_p)
-    queries = syn.LAW_C2.sample(nq, 0, 1 + rank)
-    return base, queries, graph
+    return base, rank_queries(rank, nq), graph
+
+
+def rank_queries(rank, nq=N_QUERIES):
+    """This rank's shard of the query stream: its own seeded draw from the base's law
+    (stream 1 + rank), so that no two ranks search the same queries."""
+    from parlayann_gpu_busqueda_b200 import synthetic as syn
+    return syn.LAW_C2.sample(nq, 0, 1 + rank)
+
+
+def max_over_ranks(x, device, world):
+    """The largest of every rank's x (a step time): all ranks take part in the same
+    all-reduce, so the slowest rank sets the whole job's time."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, steps, seconds):
+    """Units all ranks processed in `steps` steps over the slowest rank's time."""
+    return units_per_rank * world * steps / seconds
 
 
 def load_hnsw(pgb):
@@ -413,18 +434,10 @@ def main():
     e2e_ok = bool(np.array_equal(e_ids.numpy(), p_ids.cpu().numpy()))
 
     # ---- max over ranks ---------------------------------------------------------------
-    def worst(xs):
-        t = torch.tensor([sum(xs)], dtype=torch.float64, device=dev)
-        if world > 1:
-            import torch.distributed as dist
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    tp_ms, tb_ms, te_s = worst(t_plain), worst(t_batch), worst(e2e_t)
-    total_q = N_QUERIES * world * args.steps
-    qps_plain = total_q / (tp_ms / 1e3)
-    qps_batch = total_q / (tb_ms / 1e3)
-    qps_e2e = total_q / te_s
+    tp_ms, tb_ms, te_s = (max_over_ranks(sum(xs), dev, world) for xs in (t_plain, t_batch, e2e_t))
+    qps_plain = whole_job_rate(N_QUERIES, world, args.steps, tp_ms / 1e3)
+    qps_batch = whole_job_rate(N_QUERIES, world, args.steps, tb_ms / 1e3)
+    qps_e2e = whole_job_rate(N_QUERIES, world, args.steps, te_s)
 
     # ---- roofline of the plain kernel: algorithmic gather bytes per launch ----------
     st = p_st.cpu().numpy()
