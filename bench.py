@@ -278,16 +278,22 @@ def run_profile(args, local):
     if os.environ.get("PGB_LIB", "").endswith("libpgb_prof.so"):
         # section cycles of the batched launches only: reset, run, read
         import ctypes
-        buf = (ctypes.c_uint64 * 10)()
-        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, 10, 1))
+        names = pgb._native.SECTION_NAMES
+        nt = pgb._native.N_TIMED_SECTIONS
+        buf = (ctypes.c_uint64 * len(names))()
+        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, len(names), 1))
         for _ in range(args.steps):
             b.search(q, ids, d, st, sp)
         torch.cuda.synchronize(dev)
-        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, 10, 1))
-        cyc = list(buf)[:8]
+        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, len(names), 1))
+        cyc = list(buf)[:nt]
         tot = sum(cyc)
-        sections = {n: round(c / tot, 4) for n, c in zip(pgb._native.SECTION_NAMES, cyc)}
-        sections["cycles_per_expansion"] = tot / max(1, buf[8])
+        sections = {n: round(c / tot, 4) for n, c in zip(names, cyc)}
+        n_exp = max(1, buf[nt])
+        sections["cycles_per_expansion"] = tot / n_exp
+        # event counts per expansion
+        for n, c in zip(names[nt + 2:], list(buf)[nt + 2:]):
+            sections[n + "_per_expansion"] = round(c / n_exp, 3)
     print(json.dumps({"profile": True, "nq": nq, "Ls": Ls, "sections": sections,
                       "comps": int(stn[:, 0].astype(np.int64).sum()),
                       "expansions": int(stn[:, 1].astype(np.int64).sum()),

@@ -15,6 +15,10 @@
 //   ref_search flat <base.i8bin> <queries.i8bin> <graph> <Ls> <visit|-1> <k> <cut> <out>
 //   ref_search hnsw <base.i8bin> <queries.i8bin> <hnsw>  <Ls> <visit|-1> <k> <cut> <out>
 // out: [nq u32][k u32][ids nq*k u32][dists nq*k i32][comp nq i32][flags nq i32]
+//
+// REF_TIME_REPS=N (optional): after the checked launch, time the reference's lanzar:
+// 3 untimed launches, then N launches, each after a 512 MiB write that flushes the L2,
+// bracketed by CUDA events on the launch stream; prints one JSON line on stdout.
 
 #include <cstdio>
 #include <cstdlib>
@@ -24,6 +28,35 @@
 #include "busqueda.cuh"
 #include "hnsw.h"
 #include "lectores.h"
+
+template <class Launch>
+static void time_launches(int reps, uint32_t nq, Launch launch) {
+    const size_t flush_bytes = 512ull << 20;
+    void* flush = nullptr;
+    CHECK_CUDA(cudaMalloc(&flush, flush_bytes));
+    cudaEvent_t a, b;
+    CHECK_CUDA(cudaEventCreate(&a));
+    CHECK_CUDA(cudaEventCreate(&b));
+    for (int i = 0; i < 3; i++) launch();
+    CHECK_CUDA(cudaDeviceSynchronize());
+    double total_ms = 0;
+    for (int i = 0; i < reps; i++) {
+        CHECK_CUDA(cudaMemsetAsync(flush, i & 0xff, flush_bytes, 0));
+        CHECK_CUDA(cudaEventRecord(a, 0));
+        launch();
+        CHECK_CUDA(cudaEventRecord(b, 0));
+        CHECK_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        CHECK_CUDA(cudaEventElapsedTime(&ms, a, b));
+        total_ms += ms;
+    }
+    const double avg = total_ms / reps;
+    printf("{\"reference_kernel_ms\": %.6f, \"qps\": %.1f, \"queries\": %u, \"reps\": %d}\n", avg,
+           nq / (avg * 1e-3), nq, reps);
+    CHECK_CUDA(cudaEventDestroy(a));
+    CHECK_CUDA(cudaEventDestroy(b));
+    CHECK_CUDA(cudaFree(flush));
+}
 
 int main(int argc, char** argv) {
     if (argc != 10) {
@@ -39,6 +72,7 @@ int main(int argc, char** argv) {
     cfg.k = atoi(argv[7]);
     cfg.cut = atof(argv[8]);
     const uint32_t nq = queries.n;
+    const int reps = getenv("REF_TIME_REPS") ? atoi(getenv("REF_TIME_REPS")) : 0;
 
     VectoresGPU baseGPU, queriesGPU;
     subirVectores(base, baseGPU);
@@ -64,6 +98,7 @@ int main(int argc, char** argv) {
         b.preparar(gg, nq, cfg);
         b.lanzar(baseGPU, queriesGPU, gg, 0);
         fetch(b.idsDev, b.distsDev, b.compDev, b.banderasDev);
+        if (reps > 0) time_launches(reps, nq, [&] { b.lanzar(baseGPU, queriesGPU, gg, 0); });
         b.liberar();
         liberarGrafo(gg);
     } else if (mode == "hnsw") {
@@ -75,6 +110,7 @@ int main(int argc, char** argv) {
         b.preparar(hg, nq, cfg);
         b.lanzar(queriesGPU, hg, 0);
         fetch(b.idsDev, b.distsDev, b.compDev, b.banderasDev);
+        if (reps > 0) time_launches(reps, nq, [&] { b.lanzar(queriesGPU, hg, 0); });
         b.liberar();
         liberarHnsw(hg);
     } else {

@@ -95,7 +95,9 @@ _sig("pgb_write_graph", C.c_int, C.c_char_p, u32, u32, vp, vp)
 _sig("pgb_section_profile", C.c_int, vp, u32, C.c_int)
 _sig("pgb_file_check", C.c_int, C.c_char_p, C.c_int, vp)
 SECTION_NAMES = ["setup", "visit", "filter", "distances", "sort", "union", "shift", "cut_next",
-                 "expansions", "queries"]
+                 "expansions", "queries", "n_pending", "n_cand", "n_enter", "no_cand",
+                 "pred_hit"]
+N_TIMED_SECTIONS = 8  # the rest are event counts
 
 
 def check(status: int) -> None:

@@ -60,6 +60,11 @@ enum FlatSection {
     SEC_CUT_NEXT,    // cut, next unvisited, insert completion, prefetch
     SEC_ITERATIONS,  // (count) expansions
     SEC_QUERIES,     // (count) queries
+    SEC_N_PENDING,   // (count) rows past the lossy filter (distances computed)
+    SEC_N_CAND,      // (count) candidates under the cutoff
+    SEC_N_ENTER,     // (count) candidates entering the frontier
+    SEC_NO_CAND,     // (count) expansions with no candidate under the cutoff
+    SEC_PRED_HIT,    // (count) expansions whose row was predicted
     NUM_SECTIONS
 };
 #ifdef PGB_SECTION_PROFILE
@@ -75,11 +80,16 @@ constexpr uint32_t kProfileBytes = 8u * NUM_SECTIONS;
     do {                    \
         if (lane == 0) prof[sec] += 1ull; \
     } while (0)
+#define PGB_PROF_COUNT_N(sec, n)                                  \
+    do {                                                          \
+        if (lane == 0) prof[sec] += (unsigned long long)(n);      \
+    } while (0)
 #else
 constexpr uint32_t kProfileBytes = 0;
 #define PGB_PROF_BEGIN(t)
 #define PGB_PROF_ADD(sec, t)
 #define PGB_PROF_COUNT(sec)
+#define PGB_PROF_COUNT_N(sec, n)
 #endif
 
 struct FlatLayout {
@@ -430,6 +440,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         // whole neighbour row: the predicted one, or requested now
         uint32_t a[CH];
         if (cur == pred) {
+            PGB_PROF_COUNT(SEC_PRED_HIT);
 #pragma unroll
             for (int t = 0; t < CH; t++) a[t] = apred[t];
         } else {
@@ -531,6 +542,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
             }
         }
         comps += np;
+        PGB_PROF_COUNT_N(SEC_N_PENDING, np);
         PGB_PROF_ADD(SEC_FILTER, tp);
 
         // ---- distances ------------------------------------------------------------
@@ -554,6 +566,8 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
 
         int unew = u;
         int ne = 0;
+        PGB_PROF_COUNT_N(SEC_N_CAND, nc);
+        if (nc == 0) PGB_PROF_COUNT(SEC_NO_CAND);
         if (nc > 0) {
             sort_keys<CH>(ckey, nc, lane);
             PGB_PROF_ADD(SEC_SORT, tp);
@@ -605,6 +619,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
             }
             __syncwarp();
         }
+        PGB_PROF_COUNT_N(SEC_N_ENTER, ne);
         pred = (best != kEmptyKey) ? key_id(best) : kEmptyId;
         if (pred != kEmptyId) {
             const uint32_t* prow = A.adj + (size_t)pred * A.gs;
