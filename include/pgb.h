@@ -192,7 +192,7 @@ typedef struct pgb_batch_options {
     uint32_t exclude_query_id;
     uint32_t query_id_base;
     uint32_t warps_per_block;   /* 1, 2 or 4; 0: default (4) / tuned                    */
-    uint32_t filter_placement;  /* 0 auto, 1 shared memory, 2 global memory             */
+    uint32_t filter_placement;  /* 0 auto, 1 shared memory (max_beam <= 128), 2 global  */
     uint32_t visited_placement; /* 0 auto, 1 shared memory, 2 global memory             */
 } pgb_batch_options;
 

@@ -1,7 +1,8 @@
 // batch.cu -- pgb_batch_*: the batched persistent form of the flat-graph search.
 //
 // plan   : host step, per-query (Ls, k) -> longest-beam-first work order on the device
-// search : cudaMemsetAsync(counter) + one persistent launch (capturable)
+// search : cudaMemsetAsync(counter) + one persistent launch (capturable); a plan whose
+//          queries all share one (Ls, k) runs the uniform-batch kernel
 // tune   : times candidate (warps per block, filter / visited placement) on the planned
 //          queries and keeps the fastest; every candidate returns identical neighbours,
 //          because all of them run the same per-query code (flat_query)
@@ -30,6 +31,7 @@ struct pgb_batch {
     uint32_t* d_queue = nullptr;
     uint32_t nq = 0;
     uint32_t max_ls_planned = 0;
+    uint32_t uniform_ls = 0, uniform_k = 0;  // the plan's (Ls, k) when all queries share it
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     // host-memory path staging
@@ -112,8 +114,14 @@ pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_
     A.excl = b->opt.exclude_query_id ? 1u : 0u;
     A.qbase = b->opt.query_id_base;
     A.norm_in_row = ix->norm_in_row ? 1u : 0u;
-    A.ls_arr = b->d_ls;
-    A.k_arr = b->d_k;
+    if (b->uniform_ls) {
+        // one (Ls, k) for the whole plan: the uniform kernel reads it from A.Ls / A.k
+        A.Ls = b->uniform_ls;
+        A.k = b->uniform_k;
+    } else {
+        A.ls_arr = b->d_ls;
+        A.k_arr = b->d_k;
+    }
     A.order = b->d_order;
     A.out_stride = b->opt.max_k;
     A.ids = ids;
@@ -202,6 +210,10 @@ pgb_status pgb_batch_plan(pgb_batch* b, const uint32_t* beam_sizes, const uint32
         return s;
     b->nq = nq;
     b->max_ls_planned = mx;
+    const bool uniform = std::all_of(beam_sizes, beam_sizes + nq, [&](uint32_t v) { return v == beam_sizes[0]; }) &&
+                         std::all_of(ks, ks + nq, [&](uint32_t v) { return v == ks[0]; });
+    b->uniform_ls = uniform ? beam_sizes[0] : 0u;
+    b->uniform_k = uniform ? ks[0] : 0u;
     drop_graph(b);
     return PGB_OK;
 }

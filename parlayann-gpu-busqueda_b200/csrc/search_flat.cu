@@ -1,10 +1,6 @@
-// search_flat.cu -- the two schedules of the flat-graph beam search.
-//
-// plain   : the drop-in. Persistent grid, warp w takes queries w, w+W, ... (the
-//           reference's schedule, cuda/busqueda.cu:151-152), one Ls and k per launch.
-// batched : persistent grid whose warps pull queries from a device counter over a
-//           longest-beam-first order, each query with its own Ls and k; tables sized
-//           for the batch's largest Ls. Same per-query code, identical neighbours.
+// search_flat.cu -- launch planning for the flat-graph beam search kernels (plain and
+// batched; the kernels themselves are in search_flat_kernels.cuh, compiled per adjacency
+// chunk count by search_flat_ch*.cu).
 #include <algorithm>
 #include <cstdio>
 
@@ -12,96 +8,28 @@
 #include "search_flat.cuh"
 #include "search_plan.h"
 
-// resident 128-thread blocks per SM the flat kernels are compiled for (registers per
-// thread = 65536 / (128 * this)): 9 -> 56 registers, 36 warps per SM
-#ifndef PGB_MIN_BLOCKS
-#define PGB_MIN_BLOCKS 9
-#endif
-
 namespace pgb {
 
-#ifdef PGB_SECTION_PROFILE
-__device__ unsigned long long g_section_cycles[NUM_SECTIONS];
-// zero the warp's counters on entry, fold them into the device totals on exit
-#define PGB_PROF_ENTER()                                                                \
-    do {                                                                                \
-        if (lane < NUM_SECTIONS)                                                        \
-            reinterpret_cast<unsigned long long*>(wmem + A.L.off_prof)[lane] = 0ull;    \
-        __syncwarp();                                                                   \
-    } while (0)
-#define PGB_PROF_EXIT()                                                                 \
-    do {                                                                                \
-        __syncwarp();                                                                   \
-        if (lane < NUM_SECTIONS)                                                        \
-            atomicAdd(&g_section_cycles[lane],                                          \
-                      reinterpret_cast<unsigned long long*>(wmem + A.L.off_prof)[lane]); \
-    } while (0)
-#else
-#define PGB_PROF_ENTER()
-#define PGB_PROF_EXIT()
-#endif
-
-template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_plain_kernel(FlatArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    const uint32_t wpb = blockDim.x >> 5;
-    const uint32_t gw = blockIdx.x * wpb + w;
-    const uint32_t total = gridDim.x * wpb;
-    unsigned char* wmem = smem + (size_t)w * A.L.bytes;
-    uint32_t* gf = A.gfilter ? A.gfilter + (size_t)gw * A.gfilter_words : nullptr;
-    uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
-    PGB_PROF_ENTER();
-    for (uint32_t q = gw; q < A.nq; q += total)
-        flat_query<CH, Signed, SFILT>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
-    PGB_PROF_EXIT();
-}
-
-template <int CH, bool Signed, bool SFILT>
-__global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_batched_kernel(FlatArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    const uint32_t wpb = blockDim.x >> 5;
-    const uint32_t gw = blockIdx.x * wpb + w;
-    unsigned char* wmem = smem + (size_t)w * A.L.bytes;
-    uint32_t* gf = A.gfilter ? A.gfilter + (size_t)gw * A.gfilter_words : nullptr;
-    uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
-    PGB_PROF_ENTER();
-    for (;;) {
-        uint32_t slot = 0;
-        if (lane == 0) slot = atomicAdd(A.queue, 1u);
-        slot = __shfl_sync(kFull, slot, 0);
-        if (slot >= A.nq) break;
-        const uint32_t q = A.order[slot];
-        flat_query<CH, Signed, SFILT>(A, wmem, gf, gv, q, A.ls_arr[q], A.k_arr[q], lane);
-    }
-    PGB_PROF_EXIT();
-}
+void* flat_kernel_ch1(FlatSchedule sched, bool is_signed, uint32_t filter_words);
+void* flat_kernel_ch2(FlatSchedule sched, bool is_signed, uint32_t filter_words);
+void* flat_kernel_ch3(FlatSchedule sched, bool is_signed, uint32_t filter_words);
+void* flat_kernel_ch4(FlatSchedule sched, bool is_signed, uint32_t filter_words);
+void* flat_kernel_ch8(FlatSchedule sched, bool is_signed, uint32_t filter_words);
+cudaError_t flat_section_totals_ch1(unsigned long long* acc, bool reset);
+cudaError_t flat_section_totals_ch2(unsigned long long* acc, bool reset);
+cudaError_t flat_section_totals_ch3(unsigned long long* acc, bool reset);
+cudaError_t flat_section_totals_ch4(unsigned long long* acc, bool reset);
+cudaError_t flat_section_totals_ch8(unsigned long long* acc, bool reset);
 
 namespace {
 
-using KernelFn = void (*)(FlatArgs);
-
-template <int CH, bool Signed, bool SFILT>
-KernelFn pick_kernel(bool batched) {
-    return batched ? flat_batched_kernel<CH, Signed, SFILT> : flat_plain_kernel<CH, Signed, SFILT>;
-}
-
-template <int CH>
-KernelFn pick_ch(bool batched, bool is_signed, bool sfilt) {
-    if (is_signed) return sfilt ? pick_kernel<CH, true, true>(batched) : pick_kernel<CH, true, false>(batched);
-    return sfilt ? pick_kernel<CH, false, true>(batched) : pick_kernel<CH, false, false>(batched);
-}
-
-KernelFn pick(int ch, bool batched, bool is_signed, bool sfilt) {
+void* pick(int ch, FlatSchedule sched, bool is_signed, uint32_t filter_words) {
     switch (ch) {
-        case 1: return pick_ch<1>(batched, is_signed, sfilt);
-        case 2: return pick_ch<2>(batched, is_signed, sfilt);
-        case 3: return pick_ch<3>(batched, is_signed, sfilt);
-        case 4: return pick_ch<4>(batched, is_signed, sfilt);
-        default: return pick_ch<8>(batched, is_signed, sfilt);
+        case 1: return flat_kernel_ch1(sched, is_signed, filter_words);
+        case 2: return flat_kernel_ch2(sched, is_signed, filter_words);
+        case 3: return flat_kernel_ch3(sched, is_signed, filter_words);
+        case 4: return flat_kernel_ch4(sched, is_signed, filter_words);
+        default: return flat_kernel_ch8(sched, is_signed, filter_words);
     }
 }
 
@@ -122,13 +50,22 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     const uint32_t vwords = flat_visited_cap(ls);
     P.sfilt = rq.force_filter_placement ? rq.filter_in_shared
                                         : (4ull * fwords <= rq.filter_smem_limit);
+    // the shared-filter kernels exist for 1,024 to 4,096 words (beams up to 128)
+    if (P.sfilt && fwords > kSharedFilterMaxWords)
+        return fail(PGB_ERR_BAD_ARG, "a shared-memory filter holds at most 4,096 slots (beams up to 128)");
     P.svis = rq.force_visited_placement ? rq.visited_in_shared
                                         : (4ull * vwords <= rq.visited_smem_limit);
     const uint32_t ls_cap = (ls + 7u) & ~7u;
+    if (ls_cap > flat_fvis_cap(P.sfilt ? fwords : 0u))
+        return fail(PGB_ERR_BAD_ARG, "beam above the kernels' frontier capacity");
     P.L = make_flat_layout(ls_cap, 32u * P.ch, P.sfilt ? fwords : 0u, P.svis ? vwords : 0u);
     P.gfilter_words = P.sfilt ? 0u : fwords;
     P.gvisited_words = P.svis ? 0u : vwords;
-    P.kernel = (void*)pick(P.ch, P.batched, P.is_signed, P.sfilt);
+    const uint32_t kfw = P.sfilt ? fwords : 0u;
+    P.kernel = pick(P.ch, P.batched ? FlatSchedule::kBatched : FlatSchedule::kPlain, P.is_signed, kfw);
+    if (P.batched) P.kernel_uniform = pick(P.ch, FlatSchedule::kBatchedUniform, P.is_signed, kfw);
+    if (!P.kernel || (P.batched && !P.kernel_uniform))
+        return fail(PGB_ERR_BAD_ARG, "no kernel for this filter size");
 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return fail(PGB_ERR_CUDA, "cudaGetDevice failed");
@@ -145,15 +82,24 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     P.smem_bytes = (size_t)wpb * P.L.bytes;
     // the attribute belongs to the kernel, shared by every plan of it: set the device
     // maximum so that no later plan can shrink it under an earlier one
-    cudaError_t e = cudaFuncSetAttribute(P.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_cap);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(P.kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 (int)cudaSharedmemCarveoutMaxShared);
+    cudaError_t e = cudaSuccess;
+    for (void* kern : {P.kernel, P.kernel_uniform}) {
+        if (!kern || e != cudaSuccess) continue;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+    }
     if (e != cudaSuccess)
         return fail(PGB_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    // blocks per SM: the smaller of the two batched kernels' figures (same launch bounds)
     int bps = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, P.kernel, wpb * 32, P.smem_bytes);
+    if (e == cudaSuccess && P.kernel_uniform) {
+        int bu = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bu, P.kernel_uniform, wpb * 32, P.smem_bytes);
+        bps = std::min(bps, bu);
+    }
     if (e != cudaSuccess || bps < 1)
         return fail(PGB_ERR_CUDA, "kernel does not fit on a multiprocessor");
     if (rq.max_blocks_per_sm > 0) bps = std::min(bps, rq.max_blocks_per_sm);
@@ -172,7 +118,8 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
     int blocks = P.blocks;
     if (P.batched)
         blocks = std::max(1, std::min(blocks, (int)((A.nq + P.warps_per_block - 1) / P.warps_per_block)));
-    cudaError_t e = cudaLaunchKernel(P.kernel, dim3(blocks), dim3(P.warps_per_block * 32), args,
+    void* kern = (P.batched && !A.ls_arr) ? P.kernel_uniform : P.kernel;
+    cudaError_t e = cudaLaunchKernel(kern, dim3(blocks), dim3(P.warps_per_block * 32), args,
                                      P.smem_bytes, stream);
     if (e != cudaSuccess)
         return fail(PGB_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
@@ -184,12 +131,14 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
 extern "C" pgb_status pgb_section_profile(uint64_t* out, uint32_t n, int reset) {
 #ifdef PGB_SECTION_PROFILE
     if (!out || n < pgb::NUM_SECTIONS) return pgb::fail(PGB_ERR_BAD_ARG, "need NUM_SECTIONS slots");
-    cudaError_t e = cudaMemcpyFromSymbol(out, pgb::g_section_cycles, 8 * pgb::NUM_SECTIONS);
-    if (e == cudaSuccess && reset) {
-        unsigned long long zero[pgb::NUM_SECTIONS] = {0};
-        e = cudaMemcpyToSymbol(pgb::g_section_cycles, zero, sizeof(zero));
-    }
+    unsigned long long acc[pgb::NUM_SECTIONS] = {0};
+    cudaError_t e = pgb::flat_section_totals_ch1(acc, reset != 0);
+    if (e == cudaSuccess) e = pgb::flat_section_totals_ch2(acc, reset != 0);
+    if (e == cudaSuccess) e = pgb::flat_section_totals_ch3(acc, reset != 0);
+    if (e == cudaSuccess) e = pgb::flat_section_totals_ch4(acc, reset != 0);
+    if (e == cudaSuccess) e = pgb::flat_section_totals_ch8(acc, reset != 0);
     if (e != cudaSuccess) return pgb::fail(PGB_ERR_CUDA, cudaGetErrorString(e));
+    for (int i = 0; i < pgb::NUM_SECTIONS; i++) out[i] = acc[i];
     return PGB_OK;
 #else
     (void)out;

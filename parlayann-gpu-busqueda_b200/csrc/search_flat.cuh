@@ -92,12 +92,16 @@ constexpr uint32_t kProfileBytes = 0;
 #define PGB_PROF_COUNT_N(sec, n)
 #endif
 
+// Per-warp shared memory. Everything before the frontier keys is sized by the kernel's
+// template parameters alone (adjacency chunks, shared-filter size), so the kernel
+// addresses it with compile-time offsets; the frontier and the optional shared visited
+// table follow, sized by the plan's beam capacity.
 struct FlatLayout {
     uint32_t ls_cap;         // frontier capacity (>= largest Ls served)
-    uint32_t gs;             // adjacency row stride, multiple of 32 (>= degree limit)
+    uint32_t gs;             // adjacency entries per chunked row, 32 * chunks (>= degree limit)
     uint32_t filter_words;   // lossy filter words kept in shared memory (0: global)
     uint32_t visited_words;  // visited-table words in shared memory (0: global)
-    uint32_t off_fkey, off_fvis, off_a, off_b, off_c, off_vbits, off_filter, off_visited,
+    uint32_t off_a, off_b, off_c, off_vbits, off_filter, off_fkey, off_fvis, off_visited,
         off_prof, bytes;
 };
 
@@ -105,21 +109,26 @@ struct FlatLayout {
 // candidate whose bit is clear has never been expanded and needs no table lookup
 constexpr uint32_t kVisitedBits = 1024;  // visited_bit() yields 10 bits
 
-__host__ __device__ inline uint32_t round16(uint32_t x) { return (x + 15u) & ~15u; }
+// shared-memory lossy filters come in these sizes (words): beams up to 64, 90 and 128
+constexpr uint32_t kSharedFilterMaxWords = 4096;
 
-__host__ __device__ inline FlatLayout make_flat_layout(uint32_t ls_cap, uint32_t gs,
-                                                       uint32_t filter_words,
-                                                       uint32_t visited_words) {
-    FlatLayout L;
+// capacity of the frontier's visited bytes: the largest beam a kernel serves (128 with a
+// shared filter, PGB_MAX_BEAM otherwise), so that the region has a fixed size
+__host__ __device__ constexpr uint32_t flat_fvis_cap(uint32_t filter_words) {
+    return filter_words ? 128u : (uint32_t)PGB_MAX_BEAM;
+}
+
+__host__ __device__ constexpr uint32_t round16(uint32_t x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ constexpr FlatLayout make_flat_layout(uint32_t ls_cap, uint32_t gs,
+                                                          uint32_t filter_words,
+                                                          uint32_t visited_words) {
+    FlatLayout L{};
     L.ls_cap = ls_cap;
     L.gs = gs;
     L.filter_words = filter_words;
     L.visited_words = visited_words;
     uint32_t o = kRowBytes;  // query row at offset 0
-    L.off_fkey = o;
-    o += 8u * ls_cap;
-    L.off_fvis = o;
-    o = round16(o + ls_cap);
     L.off_a = o;  // pending ids + distances, later entering keys
     o += 8u * gs;
     L.off_b = o;  // candidate keys
@@ -128,8 +137,12 @@ __host__ __device__ inline FlatLayout make_flat_layout(uint32_t ls_cap, uint32_t
     o = round16(o + 5u * gs);
     L.off_vbits = o;
     o += kVisitedBits / 8u;
-    L.off_filter = o;
+    L.off_fvis = o;
+    o += flat_fvis_cap(filter_words);
+    L.off_filter = o;  // 16-byte aligned; its size is a multiple of 16
     o += 4u * filter_words;
+    L.off_fkey = o;  // offsets up to here depend on (gs, filter_words) only
+    o = round16(o + 8u * ls_cap);
     L.off_visited = o;
     o += 4u * visited_words;
     L.off_prof = o;
@@ -137,6 +150,10 @@ __host__ __device__ inline FlatLayout make_flat_layout(uint32_t ls_cap, uint32_t
     L.bytes = round16(o);
     return L;
 }
+
+// plain: static query striding; batched: device work queue with per-query (Ls, k);
+// batched uniform: work queue, one (Ls, k) for the whole launch
+enum class FlatSchedule { kPlain, kBatched, kBatchedUniform };
 
 struct FlatArgs {
     const uint8_t* rows;   // n x 128-byte vector rows
@@ -320,13 +337,11 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
 #pragma unroll
         for (int r = 0; r < SLOTS; r++) {
             const int i = base + r * 8 + grp;
-            va[r] = make_int4(0, 0, 0, 0);
-            vb[r] = make_int4(0, 0, 0, 0);
-            if (i < np) {
-                const uint8_t* row = rows + (size_t)ids[i] * kRowBytes + c * 16;
-                if (need_a) va[r] = ldg16(row);
-                if (need_b) vb[r] = ldg16(row + 64);
-            }
+            // slots past np re-read row ids[0] (valid and cached): every lane loads
+            // unconditionally, and those slots' sums are never stored
+            const uint8_t* row = rows + (size_t)ids[i < np ? i : 0] * kRowBytes + c * 16;
+            va[r] = need_a ? ldg16(row) : make_int4(0, 0, 0, 0);
+            vb[r] = need_b ? ldg16(row + 64) : make_int4(0, 0, 0, 0);
         }
         int32_t t[SLOTS];
         if (norm_in_row) {
@@ -366,24 +381,29 @@ __device__ __forceinline__ int32_t query_sq_norm(const int4* q4, int lane) {
 // ---- one query -----------------------------------------------------------------------
 // CH: adjacency chunks of 32. SFILT: lossy filter in shared memory (else gfilter).
 // The visited table lives in gvisited when that is non-null, else in shared memory.
-template <int CH, bool Signed, bool SFILT>
+// FW: words of the lossy filter in shared memory (1024, 2048 or 4096), 0 when it lives in
+// gfilter. Offsets up to the frontier keys are compile-time constants (K); a shared
+// visited table sits after the frontier, at the plan's offset (A.L), which the host
+// computes with the same make_flat_layout.
+template <int CH, bool Signed, int FW>
 __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfilter,
                            uint32_t* gvisited, uint32_t q, uint32_t Ls, uint32_t k, int lane) {
-    const FlatLayout& L = A.L;
+    constexpr bool SFILT = FW > 0;
+    constexpr FlatLayout K = make_flat_layout(0u, 32u * CH, (uint32_t)FW, 0u);
     uint32_t* qwords = reinterpret_cast<uint32_t*>(wmem);
-    uint64_t* fkey = reinterpret_cast<uint64_t*>(wmem + L.off_fkey);
-    uint8_t* fvis = wmem + L.off_fvis;
-    uint32_t* pend = reinterpret_cast<uint32_t*>(wmem + L.off_a);
-    int32_t* pdist = reinterpret_cast<int32_t*>(wmem + L.off_a + 4u * L.gs);
-    uint64_t* ekey = reinterpret_cast<uint64_t*>(wmem + L.off_a);  // reuses pend/pdist
-    uint64_t* ckey = reinterpret_cast<uint64_t*>(wmem + L.off_b);
-    int32_t* epos = reinterpret_cast<int32_t*>(wmem + L.off_c);
-    uint8_t* evis = wmem + L.off_c + 4u * L.gs;
-    uint32_t* filter = SFILT ? reinterpret_cast<uint32_t*>(wmem + L.off_filter) : gfilter;
-    uint32_t* vtab = gvisited ? gvisited : reinterpret_cast<uint32_t*>(wmem + L.off_visited);
-    uint32_t* vbits = reinterpret_cast<uint32_t*>(wmem + L.off_vbits);
+    uint64_t* fkey = reinterpret_cast<uint64_t*>(wmem + K.off_fkey);
+    uint8_t* fvis = wmem + K.off_fvis;
+    uint32_t* pend = reinterpret_cast<uint32_t*>(wmem + K.off_a);
+    int32_t* pdist = reinterpret_cast<int32_t*>(wmem + K.off_a + 4u * K.gs);
+    uint64_t* ekey = reinterpret_cast<uint64_t*>(wmem + K.off_a);  // reuses pend/pdist
+    uint64_t* ckey = reinterpret_cast<uint64_t*>(wmem + K.off_b);
+    int32_t* epos = reinterpret_cast<int32_t*>(wmem + K.off_c);
+    uint8_t* evis = wmem + K.off_c + 4u * K.gs;
+    uint32_t* filter = SFILT ? reinterpret_cast<uint32_t*>(wmem + K.off_filter) : gfilter;
+    uint32_t* vtab = gvisited ? gvisited : reinterpret_cast<uint32_t*>(wmem + A.L.off_visited);
+    uint32_t* vbits = reinterpret_cast<uint32_t*>(wmem + K.off_vbits);
 #ifdef PGB_SECTION_PROFILE
-    unsigned long long* prof = reinterpret_cast<unsigned long long*>(wmem + L.off_prof);
+    unsigned long long* prof = reinterpret_cast<unsigned long long*>(wmem + A.L.off_prof);
 #endif
     PGB_PROF_BEGIN(tp);
     PGB_PROF_COUNT(SEC_QUERIES);

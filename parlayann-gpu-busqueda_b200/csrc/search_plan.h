@@ -36,12 +36,14 @@ struct FlatPlan {
     int warps_per_block = 4, blocks_per_sm = 1, blocks = 1;
     uint64_t total_warps = 0;
     size_t smem_bytes = 0;
-    void* kernel = nullptr;
+    void* kernel = nullptr;          // plain, or batched with per-query (Ls, k)
+    void* kernel_uniform = nullptr;  // batched: one (Ls, k) for every query
 };
 
 int flat_chunks_for(uint32_t deg_lim);
 pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P);
-// A's table pointers must cover P.total_warps slices when the plan keeps them global
+// A's table pointers must cover P.total_warps slices when the plan keeps them global.
+// A batched launch with A.ls_arr == nullptr runs the uniform kernel on (A.Ls, A.k).
 pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream);
 
 }  // namespace pgb

@@ -88,6 +88,40 @@ def test_batch_placements_identical(pgb, golden, gpu, placement):
     assert_same("dists", dists.cpu().numpy(), want_d)
 
 
+def test_batch_uniform_and_per_query_kernels_agree(pgb, golden, gpu):
+    """A plan whose queries share one (Ls, k) runs the uniform-batch kernel; changing one
+    query's beam switches to the per-query kernel. Both give the plain search's output."""
+    import torch
+    base, queries = golden.vectors_for("vamana")
+    index = pgb.Index.flat(base, golden.graphs["vamana"])
+    nq = len(queries)
+    want = {ls: pgb.Searcher(index, nq, pgb.QueryParams(k=10, beam_size=ls)).search(queries)
+            for ls in (49, 50)}
+    q = torch.from_numpy(queries.view(np.uint8)).cuda()
+    b = pgb.Batch(index, nq, max_beam=50, max_k=10)
+    for beams in (np.full(nq, 50), np.where(np.arange(nq) == 3, 49, 50)):
+        b.plan(beams, np.full(nq, 10))
+        ids, dists, stats = b.outputs(q.device)
+        b.search(q, ids, dists, stats)
+        torch.cuda.synchronize()
+        got_i, got_d = ids.cpu().numpy().view(np.uint32), dists.cpu().numpy()
+        for qi in range(nq):
+            wi, wd, _ = want[int(beams[qi])]
+            assert_same(f"ids q{qi} Ls={beams[qi]}", got_i[qi], wi[qi])
+            assert_same(f"dists q{qi} Ls={beams[qi]}", got_d[qi], wd[qi])
+    b.close()
+    index.close()
+
+
+def test_batch_rejects_forced_shared_filter_above_4096_slots(pgb, golden, gpu):
+    base, _ = golden.vectors_for("vamana")
+    index = pgb.Index.flat(base, golden.graphs["vamana"])
+    with pytest.raises(pgb.PgbError) as e:
+        pgb.Batch(index, 16, max_beam=129, max_k=10, filter_placement=1)
+    assert "4,096 slots" in str(e.value)
+    index.close()
+
+
 def test_batch_host_path_matches_device(pgb, oracle, golden, gpu):
     base, queries = golden.vectors_for("nnd")
     graph = golden.graphs["nnd"]
