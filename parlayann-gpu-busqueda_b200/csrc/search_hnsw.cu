@@ -37,26 +37,31 @@ __host__ __device__ inline uint32_t hnsw_cap_inw(uint32_t Ls) {
 }
 
 struct HnswLayout {
-    uint32_t wcap, gs, filter_words;
+    uint32_t wcap, gs, filter_words, cap_inw;
     uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_ibits,
-        off_filter, bytes;
+        off_occ, off_filter, bytes;
 };
 
 // "maybe in is_inw" bitmap per warp: a clear bit proves absence, so most membership
 // checks never touch the global table
 constexpr uint32_t kInwBits = 4096;
 
+// The candidate list is a window ckey[c0, c0 + nC) that slides up as the closest entry is
+// popped; it is moved back to the start when an update would run past this capacity.
+__host__ __device__ inline uint32_t hnsw_ccap(uint32_t wcap) { return 2u * wcap; }
+
 __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t gs,
-                                                       uint32_t filter_words) {
+                                                       uint32_t filter_words, uint32_t cap_inw) {
     HnswLayout L;
     L.wcap = wcap;
     L.gs = gs;
     L.filter_words = filter_words;
+    L.cap_inw = cap_inw;
     uint32_t o = kRowBytes;
     L.off_w = o;
     o += 8u * wcap;
     L.off_c = o;
-    o += 8u * wcap;
+    o += 8u * hnsw_ccap(wcap);
     L.off_pend = o;
     o += 4u * gs;
     L.off_pd = o;
@@ -73,6 +78,8 @@ __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t g
     o += 4u * PGB_MAX_HNSW_ENTRIES;
     L.off_ibits = o;
     o += kInwBits / 8u;
+    L.off_occ = o;  // is_inw slot occupancy, one bit per slot (cap_inw is a power of two >= 4096)
+    o += cap_inw / 8u;
     L.off_filter = o;
     o += 4u * filter_words;
     L.bytes = round16(o);
@@ -98,46 +105,65 @@ struct HnswArgs {
     uint32_t* ids;
     int32_t* dists;
     pgb_query_stats* stats;
-    unsigned long long* inw;
+    uint32_t* inw;
     unsigned long long* gfilter;
     uint64_t epoch_base;
 };
 
+// is_inw is an exact set private to the search (only membership matters, not where ids
+// sit), so its slots come from cheap multiplicative hashes: Knuth's golden-ratio
+// constant for the home slot's top bits, a second odd constant for the maybe-bitmap.
 __device__ __forceinline__ uint32_t inw_bit(uint32_t id) {
-    return (uint32_t)(hash64_2(id) >> 48) & (kInwBits - 1u);
+    return (id * 0x85EBCA6Bu) >> (32 - 12);  // kInwBits = 4096
+}
+__device__ __forceinline__ uint32_t inw_home(uint32_t id, uint32_t shift) {
+    return (id * 0x9E3779B1u) >> shift;
 }
 
 __device__ __forceinline__ unsigned long long tag(uint32_t epoch, uint32_t id) {
     return ((unsigned long long)epoch << 32) | id;
 }
 
-// is_inw: exact set, epoch-tagged slots (a slot of an older epoch is empty)
-__device__ bool inw_contains(const unsigned long long* tab, uint32_t mask, uint32_t epoch,
-                             uint32_t id) {
-    uint32_t h = (uint32_t)(hash64_2(id) >> 32) & mask;
-    const unsigned long long want = tag(epoch, id);
+// is_inw membership: linear probing over the global id table, where a slot holds an id
+// of this layer iff its occupancy bit (shared memory, cleared per layer) is set; the
+// first clear bit of the run ends the search
+__device__ bool inw_contains(const uint32_t* tab, const uint32_t* occ, uint32_t mask,
+                             uint32_t shift, uint32_t id) {
+    uint32_t h = inw_home(id, shift);
     for (uint32_t i = 0; i <= mask; i++) {
-        const unsigned long long c = __ldcg(tab + h);
-        if (c == want) return true;
-        if ((uint32_t)(c >> 32) != epoch) return false;
+        if (!((occ[h >> 5] >> (h & 31u)) & 1u)) return false;
+        if (__ldcg(tab + h) == id) return true;
         h = (h + 1) & mask;
     }
     return false;
 }
 
-// concurrent inserts of distinct ids by several lanes
-__device__ void inw_insert(unsigned long long* tab, uint32_t mask, uint32_t epoch, uint32_t id) {
-    uint32_t h = (uint32_t)(hash64_2(id) >> 32) & mask;
-    const unsigned long long want = tag(epoch, id);
-    for (uint32_t i = 0; i <= 2 * mask + 1; i++) {
-        const unsigned long long c = __ldcg(tab + h);
-        if (c == want) return;
-        if ((uint32_t)(c >> 32) != epoch) {
-            const unsigned long long old = atomicCAS(tab + h, c, want);
-            if (old == c || old == want) return;
-            continue;  // slot taken meanwhile: look at it again
+// insert of an id known to be absent, by any number of lanes at once (distinct ids): the
+// slot is claimed with a shared-memory atomic on its occupancy bit, then written without
+// waiting; lookups come after a __syncwarp, which orders the write before them. The
+// table never fills: a layer stops (overflow) once inserts pass half of it.
+__device__ void inw_insert(uint32_t* tab, uint32_t* occ, uint32_t mask, uint32_t shift,
+                           uint32_t id) {
+    uint32_t h = inw_home(id, shift);
+    for (uint32_t i = 0; i <= mask; i++) {
+        const uint32_t bit = 1u << (h & 31u);
+        if (!(occ[h >> 5] & bit) && !(atomicOr(&occ[h >> 5], bit) & bit)) {
+            tab[h] = id;
+            return;
         }
         h = (h + 1) & mask;
+    }
+}
+
+// moves keys[from, from + n) to keys[0, n) (from >= 0; chunk reads precede chunk writes)
+__device__ __forceinline__ void slide_to_start(uint64_t* keys, int from, int n, int lane) {
+    for (int base = 0; base < n; base += 32) {
+        const int i = base + lane;
+        uint64_t v = 0;
+        if (i < n) v = keys[from + i];
+        __syncwarp();
+        if (i < n) keys[i] = v;
+        __syncwarp();
     }
 }
 
@@ -162,10 +188,13 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     uint8_t* fl = wmem + L.off_fl;
     uint32_t* eps = reinterpret_cast<uint32_t*>(wmem + L.off_eps);
     uint32_t* ibits = reinterpret_cast<uint32_t*>(wmem + L.off_ibits);
+    uint32_t* occ = reinterpret_cast<uint32_t*>(wmem + L.off_occ);
     uint32_t* sfilter = reinterpret_cast<uint32_t*>(wmem + L.off_filter);
-    unsigned long long* inw = A.inw + (size_t)gw * A.cap_inw;
+    uint32_t* inw = A.inw + (size_t)gw * A.cap_inw;
     unsigned long long* gfil = SFILT ? nullptr : A.gfilter + (size_t)gw * A.filter_slots;
     const uint32_t inw_mask = A.cap_inw - 1u;
+    const uint32_t inw_shift = 32u - (uint32_t)ceil_log2_u64(A.cap_inw);
+    const int ccap = (int)hnsw_ccap(L.wcap);
     const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
     const uint32_t layers = A.top + 1u;
 
@@ -194,8 +223,11 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             if (SFILT) {
                 for (uint32_t i = lane; i <= fmask; i += 32) sfilter[i] = kEmptyId;
             }
-            // this layer's is_inw is empty: clear its bitmap (32 lanes x 16 bytes)
+            // this layer's is_inw is empty: clear its maybe-bitmap (32 lanes x 16 bytes) and
+            // the slot occupancy bits (cap_inw / 128 16-byte words, a multiple of 32)
             reinterpret_cast<uint4*>(ibits)[lane] = make_uint4(0, 0, 0, 0);
+            for (uint32_t i = lane; i < A.cap_inw / 128u; i += 32)
+                reinterpret_cast<uint4*>(occ)[i] = make_uint4(0, 0, 0, 0);
             __syncwarp();
             // ---- entry points: distances, then the sequential inserts on lane 0 ----
             for (int e = lane; e < neps; e += 32) pend[e] = eps[e];
@@ -210,7 +242,9 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     const uint32_t s = (uint32_t)(hash64(pe) & fmask);
                     if (SFILT) sfilter[s] = pe;
                     else gfil[s] = tag(epoch, pe);
-                    inw_insert(inw, inw_mask, epoch, pe);
+                    // no membership test: a repeated entry point would take a second
+                    // slot, which changes no membership answer
+                    inw_insert(inw, occ, inw_mask, inw_shift, pe);
                     const uint32_t b = inw_bit(pe);
                     ibits[b >> 5] |= 1u << (b & 31u);
                     // cand: by distance, equal distance rejected
@@ -234,30 +268,42 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             comps += neps;
             uint32_t inserted = (uint32_t)neps;
             uint64_t cnt = 0;
-
-            while (nC > 0) {
-                if (key_dist(ckey[0]) > key_dist(wkey[nW - 1])) break;
-                if (++cnt > limit) break;
-                const uint32_t u = key_id(ckey[0]);
-                // pop the closest candidate
-                for (int base = 0; base < nC - 1; base += 32) {
-                    const int i = base + lane;
-                    uint64_t v = 0;
-                    if (i + 1 < nC) v = ckey[i + 1];
-                    __syncwarp();
-                    if (i + 1 < nC) ckey[i] = v;
-                    __syncwarp();
-                }
-                nC--;
-                exps++;
+            int c0 = 0;  // the candidate window is ckey[c0, c0 + nC)
+            // neighbour row of the next expansion, requested as soon as cand is updated
+            uint32_t unext = kEmptyId;
+            uint32_t anext[CH];
+            auto request_row = [&](uint32_t v) {
                 const uint32_t* row =
-                    (layer > 0) ? mat + ((size_t)A.upper_start[u] + (uint32_t)(layer - 1)) * stride
-                                : mat + (size_t)u * stride;
-                uint32_t a[CH];
+                    (layer > 0) ? mat + ((size_t)A.upper_start[v] + (uint32_t)(layer - 1)) * stride
+                                : mat + (size_t)v * stride;
 #pragma unroll
                 for (int t = 0; t < CH; t++) {
                     const int j = t * 32 + lane;
-                    a[t] = (j < G) ? __ldg(row + j) : kEmptyId;
+                    anext[t] = (j < G) ? __ldg(row + j) : kEmptyId;
+                }
+                unext = v;
+            };
+
+            while (nC > 0) {
+                if (key_dist(ckey[c0]) > key_dist(wkey[nW - 1])) break;
+                if (++cnt > limit) break;
+                const uint32_t u = key_id(ckey[c0]);
+                c0++;  // pop the closest candidate
+                nC--;
+                exps++;
+                uint32_t a[CH];
+                if (u == unext) {
+#pragma unroll
+                    for (int t = 0; t < CH; t++) a[t] = anext[t];
+                } else {
+                    const uint32_t* row =
+                        (layer > 0) ? mat + ((size_t)A.upper_start[u] + (uint32_t)(layer - 1)) * stride
+                                    : mat + (size_t)u * stride;
+#pragma unroll
+                    for (int t = 0; t < CH; t++) {
+                        const int j = t * 32 + lane;
+                        a[t] = (j < G) ? __ldg(row + j) : kEmptyId;
+                    }
                 }
                 // ---- lossy visited filter in row order ---------------------------------
                 int np = 0;
@@ -330,20 +376,34 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 row_distances<Signed>(A.rows, pend, pd, np, q4, qq, A.dim, A.norm_in_row != 0, lane);
 
                 // ---- eligibility: first copy in this expansion and not in is_inw ------
-                for (int j = lane; j < np; j += 32) {
-                    const uint32_t pv = pend[j];
-                    bool first = true;
-                    for (int i = 0; i < j; i++)
-                        if (pend[i] == pv) {
-                            first = false;
-                            break;
-                        }
-                    bool in_w = false;
-                    if (first) {
+                if (np <= 32) {
+                    // one chunk: earlier copies are the lanes below with the same id
+                    const uint32_t pv = lane < np ? pend[lane] : kEmptyId;
+                    const bool first = (__match_any_sync(kFull, pv) & lt) == 0;
+                    if (lane < np) {
+                        bool in_w = false;
                         const uint32_t b = inw_bit(pv);
-                        if ((ibits[b >> 5] >> (b & 31u)) & 1u) in_w = inw_contains(inw, inw_mask, epoch, pv);
+                        if (first && ((ibits[b >> 5] >> (b & 31u)) & 1u))
+                            in_w = inw_contains(inw, occ, inw_mask, inw_shift, pv);
+                        fl[lane] = (first && !in_w) ? 1 : 0;
                     }
-                    fl[j] = (first && !in_w) ? 1 : 0;
+                } else {
+                    for (int j = lane; j < np; j += 32) {
+                        const uint32_t pv = pend[j];
+                        bool first = true;
+                        for (int i = 0; i < j; i++)
+                            if (pend[i] == pv) {
+                                first = false;
+                                break;
+                            }
+                        bool in_w = false;
+                        if (first) {
+                            const uint32_t b = inw_bit(pv);
+                            if ((ibits[b >> 5] >> (b & 31u)) & 1u)
+                                in_w = inw_contains(inw, occ, inw_mask, inw_shift, pv);
+                        }
+                        fl[j] = (first && !in_w) ? 1 : 0;
+                    }
                 }
                 __syncwarp();
                 // ---- acceptance: fewer than m elements of W + earlier eligible at <= d
@@ -370,12 +430,13 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     inserted += (uint32_t)na;
                     for (int j = lane; j < na; j += 32) {
                         const uint32_t id = key_id(akey[j]);
-                        inw_insert(inw, inw_mask, epoch, id);
+                        inw_insert(inw, occ, inw_mask, inw_shift, id);
                         const uint32_t b = inw_bit(id);
                         atomicOr(&ibits[b >> 5], 1u << (b & 31u));
                     }
                     // ---- cand update (accepted keys still in arrival order) ---------------
                     const int nC0 = nC;
+                    uint64_t* cq = ckey + c0;
                     if (nC0 <= ef) {
                         // new distances only, first copy of each distance
                         int nn = 0;
@@ -386,8 +447,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                             if (j < na) {
                                 key = akey[j];
                                 const int32_t d = key_dist(key);
-                                const int p = lower_bound_key(ckey, nC0, pack_key(d, 0));
-                                nw = !(p < nC0 && key_dist(ckey[p]) == d);
+                                const int p = lower_bound_key(cq, nC0, pack_key(d, 0));
+                                nw = !(p < nC0 && key_dist(cq[p]) == d);
                                 for (int i = 0; i < j && nw; i++)
                                     if (key_dist(akey[i]) == d) nw = false;
                             }
@@ -399,8 +460,13 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         if (nn > 0) {
                             sort_keys<CH>(nkey, nn, lane);
                             const int nCn = min(ef, nC0 + nn);
+                            if (c0 + nCn > ccap) {
+                                slide_to_start(ckey, c0, nC0, lane);
+                                c0 = 0;
+                                cq = ckey;
+                            }
                             for (int j = lane; j < nn; j += 32)
-                                pos[j] = lower_bound_key(ckey, nC0, pack_key(key_dist(nkey[j]), 0)) + j;
+                                pos[j] = lower_bound_key(cq, nC0, pack_key(key_dist(nkey[j]), 0)) + j;
                             __syncwarp();
                             const int first = pos[0];
                             for (int topi = nC0 - 1; topi >= first; topi -= 32) {
@@ -409,34 +475,45 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                                 uint64_t key = 0;
                                 int np2 = 0;
                                 if (act) {
-                                    key = ckey[i];
+                                    key = cq[i];
                                     np2 = i + lower_bound_key(nkey, nn, pack_key(key_dist(key), 0));
                                 }
                                 __syncwarp();
-                                if (act && np2 < nCn) ckey[np2] = key;
+                                if (act && np2 < nCn) cq[np2] = key;
                                 __syncwarp();
                             }
                             for (int j = lane; j < nn; j += 32)
-                                if (pos[j] < nCn) ckey[pos[j]] = nkey[j];
+                                if (pos[j] < nCn) cq[pos[j]] = nkey[j];
                             __syncwarp();
                             nC = nCn;
                         }
-                    } else if (lane == 0) {
-                        // cand above ef (several top-layer entries): replay the rule
-                        for (int j = 0; j < na; j++) {
-                            const uint64_t key = akey[j];
-                            const int32_t d = key_dist(key);
-                            const int p = lower_bound_key(ckey, nC, pack_key(d, 0));
-                            if (!(p < nC && key_dist(ckey[p]) == d)) {
-                                for (int i = nC; i > p; i--) ckey[i] = ckey[i - 1];
-                                ckey[p] = key;
-                                nC++;
+                    } else {
+                        // cand above ef (several top-layer entries): replay the rule, which
+                        // holds cand at nC0 entries after each insert (one slot of headroom)
+                        if (c0 + nC0 + 1 > ccap) {
+                            slide_to_start(ckey, c0, nC0, lane);
+                            c0 = 0;
+                            cq = ckey;
+                        }
+                        if (lane == 0) {
+                            for (int j = 0; j < na; j++) {
+                                const uint64_t key = akey[j];
+                                const int32_t d = key_dist(key);
+                                const int p = lower_bound_key(cq, nC, pack_key(d, 0));
+                                if (!(p < nC && key_dist(cq[p]) == d)) {
+                                    for (int i = nC; i > p; i--) cq[i] = cq[i - 1];
+                                    cq[p] = key;
+                                    nC++;
+                                }
+                                if (nC > ef) nC--;
                             }
-                            if (nC > ef) nC--;
                         }
                     }
                     nC = __shfl_sync(kFull, nC, 0);
                     __syncwarp();
+                    // the next expansion is cand's new closest entry: request its row now,
+                    // while W is updated
+                    if (nC > 0) request_row(key_id(ckey[c0]));
                     // ---- W update: the m' smallest of W + accepted -----------------------
                     sort_keys<CH>(akey, na, lane);
                     const int nWn = min(m, nW + na);
@@ -460,6 +537,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         if (pos[j] < nWn) wkey[pos[j]] = akey[j];
                     __syncwarp();
                     nW = nWn;
+                } else if (nC > 0) {
+                    request_row(key_id(ckey[c0]));  // cand unchanged
                 }
                 if (inserted > A.cap_inw / 2) {
                     flags |= PGB_FLAG_OVERFLOW;
@@ -538,7 +617,7 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     H.sfilt = 4ull * fwords <= 4096;
     H.filter_slots = H.sfilt ? 0u : fwords;
     H.wcap = ((std::max<uint32_t>(Ls, PGB_MAX_HNSW_ENTRIES) + 8u) + 7u) & ~7u;
-    const HnswLayout L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? fwords : 0u);
+    const HnswLayout L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? fwords : 0u, H.cap_inw);
     H.warp_bytes = L.bytes;
     H.kernel = (void*)pick_hnsw(H.ch, ix->elem == PGB_INT8, H.sfilt);
     cudaDeviceProp prop;
@@ -567,9 +646,10 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     if (bps < 1) return fail(PGB_ERR_CUDA, "HNSW kernel does not fit on a multiprocessor");
     H.blocks = bps * prop.multiProcessorCount;
     H.total_warps = (uint64_t)H.blocks * wpb;
-    const size_t inw_bytes = 8ull * H.cap_inw * H.total_warps;
+    // is_inw ids; which slots hold this layer's ids is kept in shared memory, so the table
+    // needs no clearing
+    const size_t inw_bytes = 4ull * H.cap_inw * H.total_warps;
     if ((s = hnsw_cuda(cudaMalloc(&H.inw, inw_bytes), "is_inw tables")) != PGB_OK) return s;
-    if ((s = hnsw_cuda(cudaMemset(H.inw, 0, inw_bytes), "is_inw clear")) != PGB_OK) return s;
     if (!H.sfilt) {
         const size_t fb = 8ull * H.filter_slots * H.total_warps;
         if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, fb), "filter tables")) != PGB_OK) return s;
@@ -609,19 +689,17 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     A.bits0 = H.bits0;
     A.cap_inw = H.cap_inw;
     A.filter_slots = H.filter_slots;
-    A.L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? (1u << H.bits0) : 0u);
+    A.L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? (1u << H.bits0) : 0u, H.cap_inw);
     A.ids = ids;
     A.dists = dists;
     A.stats = stats;
     A.inw = H.inw;
     A.gfilter = H.gfilter;
-    // every (query, layer) of every launch gets a fresh epoch; wrap -> clear the tables
+    // every (query, layer) of every launch gets a fresh epoch for the global filter;
+    // wrap -> clear it
     const uint64_t need = (uint64_t)nq * (ix->top_level + 1ull) + 1ull;
     if (H.epoch_base + need >= 0xFFFFFFFFull) {
         pgb_status s;
-        if ((s = hnsw_cuda(cudaMemsetAsync(H.inw, 0, 8ull * H.cap_inw * H.total_warps, stream),
-                           "is_inw clear")) != PGB_OK)
-            return s;
         if (H.gfilter &&
             (s = hnsw_cuda(cudaMemsetAsync(H.gfilter, 0, 8ull * H.filter_slots * H.total_warps, stream),
                            "filter clear")) != PGB_OK)

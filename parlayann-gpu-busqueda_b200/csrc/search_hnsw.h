@@ -24,7 +24,7 @@ struct HnswState {
     uint64_t total_warps = 0;
     size_t smem_bytes = 0;
     void* kernel = nullptr;
-    unsigned long long* inw = nullptr;     // epoch-tagged exact set, per warp
+    uint32_t* inw = nullptr;               // is_inw ids per warp (slot validity in shared memory)
     unsigned long long* gfilter = nullptr; // epoch-tagged lossy filter, per warp
     uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
 };
