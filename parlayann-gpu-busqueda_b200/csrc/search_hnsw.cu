@@ -37,9 +37,9 @@ __host__ __device__ inline uint32_t hnsw_cap_inw(uint32_t Ls) {
 }
 
 struct HnswLayout {
-    uint32_t wcap, gs, filter_words, cap_inw;
+    uint32_t wcap, gs, filter_words, cap_inw, wbits_words;
     uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_ibits,
-        off_occ, off_filter, bytes;
+        off_occ, off_wbits, off_filter, bytes;
 };
 
 // "maybe in is_inw" bitmap per warp: a clear bit proves absence, so most membership
@@ -50,13 +50,17 @@ constexpr uint32_t kInwBits = 4096;
 // popped; it is moved back to the start when an update would run past this capacity.
 __host__ __device__ inline uint32_t hnsw_ccap(uint32_t wcap) { return 2u * wcap; }
 
+// filter_words: shared-memory filter (FMODE 0); wbits_words: written-slot bitmap of a
+// global id filter (FMODE 1)
 __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t gs,
-                                                       uint32_t filter_words, uint32_t cap_inw) {
+                                                       uint32_t filter_words, uint32_t cap_inw,
+                                                       uint32_t wbits_words) {
     HnswLayout L;
     L.wcap = wcap;
     L.gs = gs;
     L.filter_words = filter_words;
     L.cap_inw = cap_inw;
+    L.wbits_words = wbits_words;
     uint32_t o = kRowBytes;
     L.off_w = o;
     o += 8u * wcap;
@@ -80,6 +84,8 @@ __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t g
     o += kInwBits / 8u;
     L.off_occ = o;  // is_inw slot occupancy, one bit per slot (cap_inw is a power of two >= 4096)
     o += cap_inw / 8u;
+    L.off_wbits = o;
+    o = round16(o + 4u * wbits_words);
     L.off_filter = o;
     o += 4u * filter_words;
     L.bytes = round16(o);
@@ -167,8 +173,13 @@ __device__ __forceinline__ void slide_to_start(uint64_t* keys, int from, int n, 
     }
 }
 
-template <int CH, bool Signed, bool SFILT>
+// FMODE: where the lossy filter lives. 0: shared memory. 1: per-warp global table of ids
+// plus a shared-memory bitmap of the slots written on this layer (cleared per layer, so
+// unwritten slots need no load). 2: per-warp global table of (epoch, id) pairs, for
+// filters whose written-bitmap would not fit in shared memory.
+template <int CH, bool Signed, int FMODE>
 __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
+    constexpr bool SFILT = FMODE == 0;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -191,7 +202,10 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     uint32_t* occ = reinterpret_cast<uint32_t*>(wmem + L.off_occ);
     uint32_t* sfilter = reinterpret_cast<uint32_t*>(wmem + L.off_filter);
     uint32_t* inw = A.inw + (size_t)gw * A.cap_inw;
-    unsigned long long* gfil = SFILT ? nullptr : A.gfilter + (size_t)gw * A.filter_slots;
+    unsigned long long* gfil = FMODE == 2 ? A.gfilter + (size_t)gw * A.filter_slots : nullptr;
+    uint32_t* gf32 = FMODE == 1 ? reinterpret_cast<uint32_t*>(A.gfilter) + (size_t)gw * A.filter_slots
+                                : nullptr;
+    uint32_t* wbits = reinterpret_cast<uint32_t*>(wmem + L.off_wbits);
     const uint32_t inw_mask = A.cap_inw - 1u;
     const uint32_t inw_shift = 32u - (uint32_t)ceil_log2_u64(A.cap_inw);
     const int ccap = (int)hnsw_ccap(L.wcap);
@@ -222,6 +236,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 (uint32_t)(A.epoch_base + (uint64_t)q * layers + (A.top - (uint32_t)layer) + 1u);
             if (SFILT) {
                 for (uint32_t i = lane; i <= fmask; i += 32) sfilter[i] = kEmptyId;
+            } else if (FMODE == 1) {
+                for (uint32_t i = lane; i < (fmask + 32u) / 32u; i += 32) wbits[i] = 0u;
             }
             // this layer's is_inw is empty: clear its maybe-bitmap (32 lanes x 16 bytes) and
             // the slot occupancy bits (cap_inw / 128 16-byte words, a multiple of 32)
@@ -240,8 +256,14 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     const uint32_t pe = pend[e];
                     const int32_t d = pd[e];
                     const uint32_t s = (uint32_t)(hash64(pe) & fmask);
-                    if (SFILT) sfilter[s] = pe;
-                    else gfil[s] = tag(epoch, pe);
+                    if (SFILT) {
+                        sfilter[s] = pe;
+                    } else if (FMODE == 1) {
+                        gf32[s] = pe;
+                        wbits[s >> 5] |= 1u << (s & 31u);
+                    } else {
+                        gfil[s] = tag(epoch, pe);
+                    }
                     // no membership test: a repeated entry point would take a second
                     // slot, which changes no membership answer
                     inw_insert(inw, occ, inw_mask, inw_shift, pe);
@@ -330,14 +352,22 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         __syncwarp();
                     }
                 } else {
-                    uint32_t slot[CH];
-                    unsigned long long mem[CH];
+                    // each slot's id at the start of the row: one round of loads, skipped
+                    // (FMODE 1) for slots not written on this layer
+                    uint32_t slot[CH], mem[CH];
 #pragma unroll
                     for (int t = 0; t < CH; t++) {
                         const bool part = a[t] != kEmptyId;
                         slot[t] = part ? (uint32_t)(hash64_2(a[t]) & fmask)
                                        : (0x80000000u | (uint32_t)(t * 32 + lane));
-                        mem[t] = part ? __ldcg(gfil + slot[t]) : 0ull;
+                        mem[t] = kEmptyId;
+                        if (FMODE == 1) {
+                            if (part && ((wbits[slot[t] >> 5] >> (slot[t] & 31u)) & 1u))
+                                mem[t] = __ldcg(gf32 + slot[t]);
+                        } else if (part) {
+                            const unsigned long long m = __ldcg(gfil + slot[t]);
+                            if ((uint32_t)(m >> 32) == epoch) mem[t] = (uint32_t)m;
+                        }
                     }
                     uint32_t* sslot = reinterpret_cast<uint32_t*>(akey);
                     uint32_t* sid = sslot + 32 * CH;
@@ -353,7 +383,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         if (before) {
                             seen = part && prev == x;
                         } else {
-                            seen = part && mem[t] == tag(epoch, x);
+                            seen = part && mem[t] == x;
                             if (part)
                                 for (int p = t * 32 - 1; p >= 0; p--)
                                     if (sslot[p] == slot[t]) {
@@ -364,7 +394,14 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         __syncwarp();
                         sslot[t * 32 + lane] = slot[t];
                         sid[t * 32 + lane] = x;
-                        if (part && (peers & gt) == 0) gfil[slot[t]] = tag(epoch, x);
+                        if (part && (peers & gt) == 0) {
+                            if (FMODE == 1) {
+                                gf32[slot[t]] = x;
+                                atomicOr(&wbits[slot[t] >> 5], 1u << (slot[t] & 31u));
+                            } else {
+                                gfil[slot[t]] = tag(epoch, x);
+                            }
+                        }
                         const bool pass = part && !seen;
                         const uint32_t m = __ballot_sync(kFull, pass);
                         if (pass) pend[np + __popc(m & lt)] = x;
@@ -580,19 +617,25 @@ namespace {
 
 using HnswKernel = void (*)(HnswArgs);
 
-template <int CH>
-HnswKernel pick_hnsw_ch(bool is_signed, bool sfilt) {
-    if (is_signed) return sfilt ? hnsw_kernel<CH, true, true> : hnsw_kernel<CH, true, false>;
-    return sfilt ? hnsw_kernel<CH, false, true> : hnsw_kernel<CH, false, false>;
+template <int CH, bool Signed>
+HnswKernel pick_hnsw_mode(int fmode) {
+    return fmode == 0   ? hnsw_kernel<CH, Signed, 0>
+           : fmode == 1 ? hnsw_kernel<CH, Signed, 1>
+                        : hnsw_kernel<CH, Signed, 2>;
 }
 
-HnswKernel pick_hnsw(int ch, bool is_signed, bool sfilt) {
+template <int CH>
+HnswKernel pick_hnsw_ch(bool is_signed, int fmode) {
+    return is_signed ? pick_hnsw_mode<CH, true>(fmode) : pick_hnsw_mode<CH, false>(fmode);
+}
+
+HnswKernel pick_hnsw(int ch, bool is_signed, int fmode) {
     switch (ch) {
-        case 1: return pick_hnsw_ch<1>(is_signed, sfilt);
-        case 2: return pick_hnsw_ch<2>(is_signed, sfilt);
-        case 3: return pick_hnsw_ch<3>(is_signed, sfilt);
-        case 4: return pick_hnsw_ch<4>(is_signed, sfilt);
-        default: return pick_hnsw_ch<8>(is_signed, sfilt);
+        case 1: return pick_hnsw_ch<1>(is_signed, fmode);
+        case 2: return pick_hnsw_ch<2>(is_signed, fmode);
+        case 3: return pick_hnsw_ch<3>(is_signed, fmode);
+        case 4: return pick_hnsw_ch<4>(is_signed, fmode);
+        default: return pick_hnsw_ch<8>(is_signed, fmode);
     }
 }
 
@@ -605,6 +648,11 @@ pgb_status hnsw_cuda(cudaError_t e, const char* what) {
 
 }  // namespace
 
+HnswLayout hnsw_layout_of(const HnswState& H) {
+    return make_hnsw_layout(H.wcap, 32u * H.ch, H.fmode == 0 ? (1u << H.bits0) : 0u, H.cap_inw,
+                            H.fmode == 1 ? H.filter_slots / 32u : 0u);
+}
+
 pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswState& H) {
     H = HnswState{};
     const uint32_t Ls = p.beam_size;
@@ -613,13 +661,15 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     H.cap_inw = hnsw_cap_inw(Ls);
     const uint32_t fwords = 1u << H.bits0;
     // shared-memory filter only while small (Ls <= 64): a 16 KB filter would cap the
-    // kernel at 8 resident warps per SM; larger ones use the epoch-tagged global table
-    H.sfilt = 4ull * fwords <= 4096;
-    H.filter_slots = H.sfilt ? 0u : fwords;
+    // kernel at 8 resident warps per SM. Up to 16,384 slots (Ls <= 256) the global table
+    // holds bare ids beside a written-slot bitmap in shared memory (2 KB at most); larger
+    // filters use (epoch, id) pairs.
+    H.fmode = 4ull * fwords <= 4096 ? 0 : (fwords <= 16384 ? 1 : 2);
+    H.filter_slots = H.fmode ? fwords : 0u;
     H.wcap = ((std::max<uint32_t>(Ls, PGB_MAX_HNSW_ENTRIES) + 8u) + 7u) & ~7u;
-    const HnswLayout L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? fwords : 0u, H.cap_inw);
+    const HnswLayout L = hnsw_layout_of(H);
     H.warp_bytes = L.bytes;
-    H.kernel = (void*)pick_hnsw(H.ch, ix->elem == PGB_INT8, H.sfilt);
+    H.kernel = (void*)pick_hnsw(H.ch, ix->elem == PGB_INT8, H.fmode);
     cudaDeviceProp prop;
     int dev = 0;
     pgb_status s;
@@ -650,7 +700,11 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     // needs no clearing
     const size_t inw_bytes = 4ull * H.cap_inw * H.total_warps;
     if ((s = hnsw_cuda(cudaMalloc(&H.inw, inw_bytes), "is_inw tables")) != PGB_OK) return s;
-    if (!H.sfilt) {
+    if (H.fmode == 1) {  // ids only; validity is the shared written-slot bitmap
+        if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, 4ull * H.filter_slots * H.total_warps),
+                           "filter tables")) != PGB_OK)
+            return s;
+    } else if (H.fmode == 2) {
         const size_t fb = 8ull * H.filter_slots * H.total_warps;
         if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, fb), "filter tables")) != PGB_OK) return s;
         if ((s = hnsw_cuda(cudaMemset(H.gfilter, 0, fb), "filter clear")) != PGB_OK) return s;
@@ -689,18 +743,18 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     A.bits0 = H.bits0;
     A.cap_inw = H.cap_inw;
     A.filter_slots = H.filter_slots;
-    A.L = make_hnsw_layout(H.wcap, 32u * H.ch, H.sfilt ? (1u << H.bits0) : 0u, H.cap_inw);
+    A.L = hnsw_layout_of(H);
     A.ids = ids;
     A.dists = dists;
     A.stats = stats;
     A.inw = H.inw;
     A.gfilter = H.gfilter;
-    // every (query, layer) of every launch gets a fresh epoch for the global filter;
-    // wrap -> clear it
+    // every (query, layer) of every launch gets a fresh epoch for an (epoch, id) global
+    // filter; wrap -> clear it
     const uint64_t need = (uint64_t)nq * (ix->top_level + 1ull) + 1ull;
     if (H.epoch_base + need >= 0xFFFFFFFFull) {
         pgb_status s;
-        if (H.gfilter &&
+        if (H.fmode == 2 &&
             (s = hnsw_cuda(cudaMemsetAsync(H.gfilter, 0, 8ull * H.filter_slots * H.total_warps, stream),
                            "filter clear")) != PGB_OK)
             return s;

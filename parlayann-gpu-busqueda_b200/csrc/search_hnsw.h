@@ -14,7 +14,7 @@ namespace pgb {
 struct HnswState {
     bool ready = false;
     int ch = 1;
-    bool sfilt = true;
+    int fmode = 0;              // lossy filter: 0 shared, 1 global ids + shared bitmap, 2 global (epoch, id)
     uint32_t bits0 = 2;         // layer-0 filter bits
     uint32_t cap_inw = 0;       // is_inw slots (power of two)
     uint32_t filter_slots = 0;  // global filter slots per warp (0: shared)
@@ -25,7 +25,8 @@ struct HnswState {
     size_t smem_bytes = 0;
     void* kernel = nullptr;
     uint32_t* inw = nullptr;               // is_inw ids per warp (slot validity in shared memory)
-    unsigned long long* gfilter = nullptr; // epoch-tagged lossy filter, per warp
+    unsigned long long* gfilter = nullptr; // global lossy filter per warp: 4-byte ids
+                                           // (fmode 1) or (epoch, id) pairs (fmode 2)
     uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
 };
 
