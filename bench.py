@@ -36,6 +36,7 @@ N_QUERIES = 29_316
 K = 10
 R, L_BUILD, ALPHA = 64, 128, 1.2
 TARGET_RECALL = 0.90
+POLL_HEAD = 4096  # serving client: outstanding tickets polled per pass, oldest first
 METRIC = "QPS @ recall@10=0.90, batched vs plain kernel, 1 B200; serving p50/p99 latency"
 
 
@@ -686,29 +687,44 @@ def run_serving(args, local):
         gaps = rng.exponential(mean_burst / rate, n_events)
         sizes = np.where(rng.random(n_events) < 0.5, 1, rng.integers(2, 257, n_events))
         t_evt = np.cumsum(gaps)
-        outstanding, issued, done_q, recalls = [], 0, 0, []
+        # every request's query, beam and k drawn before the clock starts: event e submits
+        # rows off[e]:off[e+1] of these arrays (contiguous views, no copies in the loop)
+        off = np.concatenate([[0], np.cumsum(sizes)])
+        sel_all = rng.integers(0, N_QUERIES, int(off[-1]))
+        q_all = np.ascontiguousarray(queries[sel_all])
+        L_all = rng.choice(np.array([20, 50, 100, 300], np.uint32), int(off[-1]))
+        k_all = rng.choice(np.array([10, 100], np.uint32), int(off[-1]))
+        # outstanding tickets in submission order; each pass polls the oldest POLL_HEAD of
+        # them (batches complete roughly in launch order), so the client's own work stays
+        # bounded when the server is saturated and the pool holds thousands of requests
+        out_t, out_q = np.empty(0, np.uint64), np.empty(0, np.int64)
+        new_t, new_q = [], []
+        issued, done_q, recalls = 0, 0, []
         t0 = time.perf_counter()
         ev = 0
-        while ev < n_events or outstanding:
+        while ev < n_events or len(out_t) or new_t:
             now = time.perf_counter() - t0
             while ev < n_events and t_evt[ev] <= now:
-                m = int(sizes[ev])
-                sel = rng.integers(0, N_QUERIES, m)
-                L = rng.choice(np.array([20, 50, 100, 300], np.uint32), m)
-                k = rng.choice(np.array([10, 100], np.uint32), m)
-                t = srv.submit_many(queries[sel], L, k)
-                outstanding.append((t, sel[:len(t)]))
+                a, b = int(off[ev]), int(off[ev + 1])
+                t = srv.submit_many(q_all[a:b], L_all[a:b], k_all[a:b])
+                if len(t):
+                    new_t.append(t)
+                    new_q.append(sel_all[a:a + len(t)])
                 issued += len(t)
                 ev += 1
-            if outstanding:
-                tk = np.concatenate([o[0] for o in outstanding])
-                qs = np.concatenate([o[1] for o in outstanding])
-                done, oi, _, _ = srv.poll_many(tk)
+            if new_t:
+                out_t = np.concatenate([out_t] + new_t)
+                out_q = np.concatenate([out_q] + new_q)
+                new_t, new_q = [], []
+            if len(out_t):
+                head_t, head_q = out_t[:POLL_HEAD], out_q[:POLL_HEAD]
+                done, oi, _, _ = srv.poll_many(head_t)
                 if done.any():
-                    rec = pgb.recall(gt_ids[qs[done]], gt_d[qs[done]], oi[done][:, :K], K)
+                    rec = pgb.recall(gt_ids[head_q[done]], gt_d[head_q[done]], oi[done][:, :K], K)
                     recalls.append((rec, int(done.sum())))
                     done_q += int(done.sum())
-                    outstanding = [(tk[~done], qs[~done])] if (~done).any() else []
+                    out_t = np.concatenate([head_t[~done], out_t[POLL_HEAD:]])
+                    out_q = np.concatenate([head_q[~done], out_q[POLL_HEAD:]])
             if now > 20 * seconds:
                 break
         wall = time.perf_counter() - t0

@@ -8,16 +8,25 @@
 // download per output array. New arrivals therefore start while earlier launches are
 // still on the GPU, and their work overlaps on the device. Every request runs the same
 // per-query code as the plain searcher, so its answer does not depend on the mix.
+//
+// Locking: one mutex guards the pending queue, the free-slot list, the counters and the
+// contexts' busy state, and is held only for those short updates. Packing, launching and
+// copying results run outside it. A ticket names its slot (generation << 32 | slot);
+// a slot's results are published through its atomic `done` flag and collected by
+// whichever poll retires the ticket (compare-and-swap to 0), so polls take the lock only
+// to return freed slots. Under overload the GPU keeps running at its own rate while the
+// excess requests are refused (PGB_ERR_BUSY).
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <numeric>
 #include <string>
 #include <thread>
-#include <unordered_map>
 #include <vector>
 
 #include "errors.h"
@@ -31,10 +40,11 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 struct Slot {
-    uint64_t ticket = 0;
+    std::atomic<uint64_t> ticket{0};  // the live ticket, 0 when free or collected
+    std::atomic<bool> done{false};    // results below are complete
+    uint32_t gen = 0;                 // generation of the last ticket issued here
     uint32_t Ls = 0, k = 0;
     Clock::time_point t_submit;
-    bool done = false;
     std::vector<uint8_t> query;
     std::vector<uint32_t> ids;
     std::vector<int32_t> dists;
@@ -45,7 +55,7 @@ struct Slot {
 struct Context {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
-    bool busy = false;
+    bool busy = false;            // written by the dispatcher under the lock
     std::vector<uint32_t> slots;  // pool slots, batch-local order
     uint8_t* h_in = nullptr;      // pinned: queries | ls | k | order
     uint32_t* h_ids = nullptr;
@@ -72,11 +82,10 @@ struct pgb_server {
     uint32_t deg_lim = 0;
     size_t in_q_bytes = 0, in_bytes = 0;  // staging layout
     std::vector<pgb::Context> ctx;
-    std::vector<pgb::Slot> pool;
+    std::unique_ptr<pgb::Slot[]> pool;
+    uint32_t pool_n = 0;
     std::vector<uint32_t> free_slots;
     std::deque<uint32_t> pending;
-    std::unordered_map<uint64_t, uint32_t> by_ticket;
-    uint64_t next_ticket = 1;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
     std::thread dispatcher;
@@ -142,6 +151,7 @@ size_t context_device_bytes(const pgb_server* S) {
            4ull * (S->plan.gfilter_words + S->plan.gvisited_words) * tw;
 }
 
+// called with the lock held
 void set_failed(pgb_server* S, pgb_status s, const std::string& m) {
     if (S->failed == PGB_OK) {
         S->failed = s;
@@ -150,13 +160,17 @@ void set_failed(pgb_server* S, pgb_status s, const std::string& m) {
     S->cv_done.notify_all();
 }
 
-// called with the lock held
-void launch(pgb_server* S, Context& c) {
+void fail_unlocked(pgb_server* S, pgb_status s, const std::string& m) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    set_failed(S, s, m);
+}
+
+// packs c.slots (taken from the pending queue under the lock) and launches them; runs
+// without the lock: pending slots are not touched by anyone else until they are done
+bool launch(pgb_server* S, Context& c) {
     const pgb_index* ix = S->index;
     const size_t mb = S->opt.max_batch;
-    const uint32_t b = (uint32_t)std::min<size_t>(mb, S->pending.size());
-    c.slots.assign(S->pending.begin(), S->pending.begin() + b);
-    S->pending.erase(S->pending.begin(), S->pending.begin() + b);
+    const uint32_t b = (uint32_t)c.slots.size();
     uint32_t* ls = reinterpret_cast<uint32_t*>(c.h_in + S->in_q_bytes);
     uint32_t* ks = ls + mb;
     uint32_t* order = ks + mb;
@@ -172,8 +186,8 @@ void launch(pgb_server* S, Context& c) {
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d_queue, 0, 4, c.stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        set_failed(S, PGB_ERR_CUDA, std::string("server upload: ") + cudaGetErrorString(e));
-        return;
+        fail_unlocked(S, PGB_ERR_CUDA, std::string("server upload: ") + cudaGetErrorString(e));
+        return false;
     }
     FlatArgs A{};
     A.rows = ix->rows;
@@ -202,8 +216,8 @@ void launch(pgb_server* S, Context& c) {
     A.gvisited = c.gvisited;
     A.queue = c.d_queue;
     if (launch_flat(S->plan, A, c.stream) != PGB_OK) {
-        set_failed(S, PGB_ERR_CUDA, pgb_last_error());
-        return;
+        fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
+        return false;
     }
     const size_t mk = S->opt.max_k;
     e = cudaMemcpyAsync(c.h_ids, c.d_ids, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
@@ -215,79 +229,91 @@ void launch(pgb_server* S, Context& c) {
     if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        set_failed(S, PGB_ERR_CUDA, std::string("server launch: ") + cudaGetErrorString(e));
-        return;
+        fail_unlocked(S, PGB_ERR_CUDA, std::string("server launch: ") + cudaGetErrorString(e));
+        return false;
     }
-    c.busy = true;
-    S->launches++;
-    S->launched_requests += b;
+    return true;
 }
 
-// called with the lock held
-void finish(pgb_server* S, Context& c) {
+// publishes a finished launch: results into the slots (no lock), then counters
+void finish(pgb_server* S, Context& c, std::vector<float>& lat) {
     const size_t mk = S->opt.max_k;
     const auto now = Clock::now();
+    lat.clear();
     for (size_t j = 0; j < c.slots.size(); j++) {
         Slot& sl = S->pool[c.slots[j]];
         std::copy(c.h_ids + j * mk, c.h_ids + j * mk + sl.k, sl.ids.begin());
         std::copy(c.h_dists + j * mk, c.h_dists + j * mk + sl.k, sl.dists.begin());
         sl.stats = c.h_stats[j];
-        sl.done = true;
-        const float us = std::chrono::duration<float, std::micro>(now - sl.t_submit).count();
-        S->lat_us[S->lat_pos] = us;
-        S->lat_pos = (S->lat_pos + 1) % kLatencyRing;
-        if (S->lat_pos == 0) S->lat_full = true;
-        S->completed++;
+        lat.push_back(std::chrono::duration<float, std::micro>(now - sl.t_submit).count());
+        sl.done.store(true, std::memory_order_release);
     }
-    c.slots.clear();
-    c.busy = false;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        for (float us : lat) {
+            S->lat_us[S->lat_pos] = us;
+            S->lat_pos = (S->lat_pos + 1) % kLatencyRing;
+            if (S->lat_pos == 0) S->lat_full = true;
+        }
+        S->completed += lat.size();
+        c.slots.clear();
+        c.busy = false;
+    }
     S->cv_done.notify_all();
 }
 
 void dispatch_loop(pgb_server* S) {
     cudaSetDevice(S->index->device);
-    std::unique_lock<std::mutex> lk(S->mu);
+    std::vector<float> lat;
     for (;;) {
         bool progressed = false;
         int inflight = 0;
         for (Context& c : S->ctx) {
-            if (!c.busy) continue;
+            if (!c.busy) continue;  // only this thread changes busy
             const cudaError_t q = cudaEventQuery(c.done);
             if (q == cudaSuccess) {
-                finish(S, c);
+                finish(S, c, lat);
                 progressed = true;
             } else if (q != cudaErrorNotReady) {
                 cudaGetLastError();
+                std::lock_guard<std::mutex> lk(S->mu);
                 set_failed(S, PGB_ERR_CUDA, std::string("server kernel: ") + cudaGetErrorString(q));
                 c.busy = false;
             } else {
                 inflight++;
             }
         }
-        if (S->failed == PGB_OK) {
-            for (Context& c : S->ctx) {
-                if (c.busy || S->pending.empty()) continue;
+        for (Context& c : S->ctx) {
+            if (c.busy) continue;
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                if (S->failed != PGB_OK || S->pending.empty()) break;
                 // while other launches run, a partial batch may wait a little to grow
                 if (inflight > 0 && S->opt.max_wait_us > 0 && S->pending.size() < S->opt.max_batch) {
                     const auto age = Clock::now() - S->pool[S->pending.front()].t_submit;
                     if (age < std::chrono::microseconds(S->opt.max_wait_us)) break;
                 }
-                launch(S, c);
-                if (S->failed != PGB_OK) break;
-                inflight++;
-                progressed = true;
+                const size_t b = std::min<size_t>(S->opt.max_batch, S->pending.size());
+                c.slots.assign(S->pending.begin(), S->pending.begin() + b);
+                S->pending.erase(S->pending.begin(), S->pending.begin() + b);
+                c.busy = true;
+                S->launches++;
+                S->launched_requests += b;
             }
-        }
-        if (S->stop && (S->pending.empty() || S->failed != PGB_OK) && inflight == 0) break;
-        if (!progressed) {
-            if (inflight > 0) {
-                lk.unlock();
-                std::this_thread::yield();
-                lk.lock();
-            } else {
-                S->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+            if (!launch(S, c)) {
+                std::lock_guard<std::mutex> lk(S->mu);
+                c.busy = false;
+                break;
             }
+            inflight++;
+            progressed = true;
         }
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            if (S->stop && (S->pending.empty() || S->failed != PGB_OK) && inflight == 0) break;
+            if (!progressed && inflight == 0) S->cv_work.wait_for(lk, std::chrono::milliseconds(2));
+        }
+        if (!progressed && inflight > 0) std::this_thread::yield();
     }
 }
 
@@ -304,6 +330,43 @@ void destroy_server(pgb_server* S) {
         free_context(c);
     }
     delete S;
+}
+
+// called with the lock held; the pool has a free slot
+uint64_t admit(pgb_server* S, const uint8_t* query, uint32_t beam_size, uint32_t k,
+               Clock::time_point now) {
+    const uint32_t slot = S->free_slots.back();
+    S->free_slots.pop_back();
+    Slot& sl = S->pool[slot];
+    memcpy(sl.query.data(), query, S->index->dim);
+    sl.Ls = beam_size;
+    sl.k = k;
+    sl.t_submit = now;
+    sl.gen++;
+    if (sl.gen == 0) sl.gen = 1;  // tickets are never 0
+    const uint64_t ticket = ((uint64_t)sl.gen << 32) | slot;
+    sl.done.store(false, std::memory_order_relaxed);
+    sl.ticket.store(ticket, std::memory_order_release);
+    S->pending.push_back(slot);
+    return ticket;
+}
+
+// the slot of a live ticket, or nullptr
+Slot* slot_of(pgb_server* S, uint64_t ticket) {
+    const uint32_t slot = (uint32_t)ticket;
+    if (ticket == 0 || slot >= S->pool_n) return nullptr;
+    Slot& sl = S->pool[slot];
+    return sl.ticket.load(std::memory_order_acquire) == ticket ? &sl : nullptr;
+}
+
+// retires a done ticket (one caller wins) and copies its results out
+bool collect(Slot& sl, uint64_t ticket, uint32_t* ids, int32_t* dists, pgb_query_stats* stats) {
+    uint64_t expect = ticket;
+    if (!sl.ticket.compare_exchange_strong(expect, 0, std::memory_order_acq_rel)) return false;
+    std::copy(sl.ids.begin(), sl.ids.begin() + sl.k, ids);
+    std::copy(sl.dists.begin(), sl.dists.begin() + sl.k, dists);
+    if (stats) *stats = sl.stats;
+    return true;
 }
 
 }  // namespace
@@ -363,14 +426,14 @@ pgb_status pgb_server_create(pgb_index* ix, const pgb_server_options* opt, pgb_s
             return s;
         }
     // pool: every context's batch in flight plus as many waiting
-    const size_t slots = 2 * S->ctx.size() * mb;
-    S->pool.resize(slots);
-    for (Slot& sl : S->pool) {
-        sl.query.resize(ix->dim);
-        sl.ids.resize(S->opt.max_k);
-        sl.dists.resize(S->opt.max_k);
+    S->pool_n = (uint32_t)(2 * S->ctx.size() * mb);
+    S->pool.reset(new Slot[S->pool_n]);
+    for (uint32_t i = 0; i < S->pool_n; i++) {
+        S->pool[i].query.resize(ix->dim);
+        S->pool[i].ids.resize(S->opt.max_k);
+        S->pool[i].dists.resize(S->opt.max_k);
     }
-    S->free_slots.resize(slots);
+    S->free_slots.resize(S->pool_n);
     std::iota(S->free_slots.rbegin(), S->free_slots.rend(), 0u);
     S->lat_us.assign(kLatencyRing, 0.f);
     S->dispatcher = std::thread(dispatch_loop, S);
@@ -391,19 +454,8 @@ pgb_status pgb_server_submit(pgb_server* S, const void* query, uint32_t beam_siz
             S->rejected++;
             return fail(PGB_ERR_BUSY, "request pool full");
         }
-        const uint32_t slot = S->free_slots.back();
-        S->free_slots.pop_back();
-        Slot& sl = S->pool[slot];
-        memcpy(sl.query.data(), query, S->index->dim);
-        sl.Ls = beam_size;
-        sl.k = k;
-        sl.done = false;
-        sl.ticket = S->next_ticket++;
-        sl.t_submit = Clock::now();
-        S->by_ticket[sl.ticket] = slot;
-        S->pending.push_back(slot);
+        *ticket = admit(S, static_cast<const uint8_t*>(query), beam_size, k, Clock::now());
         S->submitted++;
-        *ticket = sl.ticket;
     }
     S->cv_work.notify_one();
     return PGB_OK;
@@ -412,24 +464,24 @@ pgb_status pgb_server_submit(pgb_server* S, const void* query, uint32_t beam_siz
 pgb_status pgb_server_poll(pgb_server* S, uint64_t ticket, uint32_t timeout_us, uint32_t* ids,
                            int32_t* dists, pgb_query_stats* stats) {
     if (!S || !ids || !dists) return fail(PGB_ERR_BAD_ARG, "null argument");
-    std::unique_lock<std::mutex> lk(S->mu);
-    auto it = S->by_ticket.find(ticket);
-    if (it == S->by_ticket.end()) return fail(PGB_ERR_NOT_FOUND, "unknown ticket");
-    const uint32_t slot = it->second;
-    Slot& sl = S->pool[slot];
-    if (!sl.done) {
-        S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us),
-                            [&] { return sl.done || S->failed != PGB_OK; });
+    Slot* sl = slot_of(S, ticket);
+    if (!sl) return fail(PGB_ERR_NOT_FOUND, "unknown ticket");
+    if (!sl->done.load(std::memory_order_acquire)) {
+        std::unique_lock<std::mutex> lk(S->mu);
+        S->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), [&] {
+            return sl->done.load(std::memory_order_acquire) || S->failed != PGB_OK ||
+                   sl->ticket.load(std::memory_order_acquire) != ticket;
+        });
+        if (sl->ticket.load(std::memory_order_acquire) != ticket)
+            return fail(PGB_ERR_NOT_FOUND, "unknown ticket");
+        if (!sl->done.load(std::memory_order_acquire)) {
+            if (S->failed != PGB_OK) return fail(S->failed, S->fail_msg);
+            return fail(PGB_ERR_TIMEOUT, "request not finished");
+        }
     }
-    if (!sl.done) {
-        if (S->failed != PGB_OK) return fail(S->failed, S->fail_msg);
-        return fail(PGB_ERR_TIMEOUT, "request not finished");
-    }
-    std::copy(sl.ids.begin(), sl.ids.begin() + sl.k, ids);
-    std::copy(sl.dists.begin(), sl.dists.begin() + sl.k, dists);
-    if (stats) *stats = sl.stats;
-    S->by_ticket.erase(it);
-    S->free_slots.push_back(slot);
+    if (!collect(*sl, ticket, ids, dists, stats)) return fail(PGB_ERR_NOT_FOUND, "unknown ticket");
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->free_slots.push_back((uint32_t)ticket);
     return PGB_OK;
 }
 
@@ -452,20 +504,8 @@ pgb_status pgb_server_submit_many(pgb_server* S, const void* queries, uint32_t n
         if (S->stop) return fail(PGB_ERR_BAD_ARG, "server is shutting down");
         const auto now = Clock::now();
         const uint8_t* q = static_cast<const uint8_t*>(queries);
-        for (; got < n && !S->free_slots.empty(); got++) {
-            const uint32_t slot = S->free_slots.back();
-            S->free_slots.pop_back();
-            Slot& sl = S->pool[slot];
-            memcpy(sl.query.data(), q + (size_t)got * query_stride, S->index->dim);
-            sl.Ls = beam_sizes[got];
-            sl.k = ks[got];
-            sl.done = false;
-            sl.ticket = S->next_ticket++;
-            sl.t_submit = now;
-            S->by_ticket[sl.ticket] = slot;
-            S->pending.push_back(slot);
-            tickets[got] = sl.ticket;
-        }
+        for (; got < n && !S->free_slots.empty(); got++)
+            tickets[got] = admit(S, q + (size_t)got * query_stride, beam_sizes[got], ks[got], now);
         S->submitted += got;
         S->rejected += n - got;
     }
@@ -481,25 +521,20 @@ pgb_status pgb_server_poll_many(pgb_server* S, const uint64_t* tickets, uint32_t
     if (!S || !tickets || !ids || !dists || !done || !n_done)
         return fail(PGB_ERR_BAD_ARG, "null argument");
     const size_t mk = S->opt.max_k;
-    uint32_t cnt = 0;
-    std::lock_guard<std::mutex> lk(S->mu);
+    std::vector<uint32_t> freed;
     for (uint32_t i = 0; i < n; i++) {
         done[i] = 0;
-        auto it = S->by_ticket.find(tickets[i]);
-        if (it == S->by_ticket.end()) continue;
-        const uint32_t slot = it->second;
-        Slot& sl = S->pool[slot];
-        if (!sl.done) continue;
-        std::copy(sl.ids.begin(), sl.ids.begin() + sl.k, ids + i * mk);
-        std::copy(sl.dists.begin(), sl.dists.begin() + sl.k, dists + i * mk);
-        if (stats) stats[i] = sl.stats;
-        S->by_ticket.erase(it);
-        S->free_slots.push_back(slot);
+        Slot* sl = slot_of(S, tickets[i]);
+        if (!sl || !sl->done.load(std::memory_order_acquire)) continue;
+        if (!collect(*sl, tickets[i], ids + i * mk, dists + i * mk, stats ? stats + i : nullptr))
+            continue;
+        freed.push_back((uint32_t)tickets[i]);
         done[i] = 1;
-        cnt++;
     }
-    *n_done = cnt;
-    if (S->failed != PGB_OK && cnt == 0) return fail(S->failed, S->fail_msg);
+    *n_done = (uint32_t)freed.size();
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->free_slots.insert(S->free_slots.end(), freed.begin(), freed.end());
+    if (S->failed != PGB_OK && freed.empty()) return fail(S->failed, S->fail_msg);
     return PGB_OK;
 }
 
@@ -516,11 +551,11 @@ pgb_status pgb_server_get_stats(pgb_server* S, pgb_server_stats* out) {
         uint32_t inflight = 0;
         for (const Context& c : S->ctx) inflight += c.busy ? (uint32_t)c.slots.size() : 0u;
         out->in_flight = inflight;
-        out->pool_slots = (uint32_t)S->pool.size();
+        out->pool_slots = S->pool_n;
         out->streams = (uint32_t)S->ctx.size();
         out->mean_batch = S->launches ? (double)S->launched_requests / S->launches : 0.0;
-        const size_t n = S->lat_full ? kLatencyRing : S->lat_pos;
-        lat.assign(S->lat_us.begin(), S->lat_us.begin() + n);
+        const size_t nl = S->lat_full ? kLatencyRing : S->lat_pos;
+        lat.assign(S->lat_us.begin(), S->lat_us.begin() + nl);
     }
     out->p50_us = out->p99_us = 0;
     if (!lat.empty()) {
