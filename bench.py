@@ -314,18 +314,20 @@ def main():
     ap.add_argument("--profile-nq", type=int, default=8192)
     ap.add_argument("--profile-ls", type=int, default=40)
     ap.add_argument("--workload", default="vamana",
-                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving"],
+                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving", "c4"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
                          "mixed: 100k queries of uneven Ls and k in one launch; serving: "
-                         "Poisson bursts through the request loop")
+                         "Poisson bursts through the request loop; c4: 10M uint8 d=128 "
+                         "Vamana, 100k queries, Ls 20/50/100/200")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.profile:
         run_profile(args, local)
         return
-    if args.workload in ("hnsw", "mixed", "serving") and args.impl == "ours":
-        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving}[args.workload](args, local)
+    if args.workload in ("hnsw", "mixed", "serving", "c4") and args.impl == "ours":
+        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving,
+         "c4": run_c4}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -602,6 +604,105 @@ def run_hnsw(args, local):
                      "frac": achieved / peak, "traffic": None, "peak_source": kind,
                      "kernel": "hnsw_kernel"},
         "gpu_launches": args.steps}), flush=True)
+
+
+C4_N, C4_NQ, C4_LS = 10_000_000, 100_000, (20, 50, 100, 200)
+
+
+def load_c4(pgb):
+    """10M uint8 d=128 base (4,096-centre law, 40 % zeros) and its Vamana R=64 L=128
+    alpha=1.2 graph, generated and built once, cached on disk."""
+    from parlayann_gpu_busqueda_b200.synthetic import LAW_C4
+    base_p = os.path.join(data_dir(), "c4_base.u8bin")
+    graph_p = os.path.join(data_dir(), "c4_vamana_R64_L128_a1.2.graph")
+    if not os.path.exists(base_p):
+        t = time.time()
+        base = LAW_C4.sample(C4_N, 0, 0)
+        pgb.write_vectors(base_p + ".tmp", base)
+        os.replace(base_p + ".tmp", base_p)
+        log(f"generated C4 base in {time.time() - t:.1f} s")
+    base = pgb.read_vectors(base_p, np.uint8)
+    if not os.path.exists(graph_p):
+        t = time.time()
+        g = pgb.build_vamana(base, R=R, L=L_BUILD, alpha=ALPHA, seed=0)
+        pgb.write_graph(graph_p + ".tmp", g)
+        os.replace(graph_p + ".tmp", graph_p)
+        log(f"built C4 Vamana 10M in {time.time() - t:.1f} s")
+    return base, pgb.read_graph(graph_p), LAW_C4.sample(C4_NQ, 0, 1)
+
+
+def run_c4(args, local):
+    """Scale: 10M uint8 d=128 rows (1.28 GB) + Vamana R=64 (2.56 GB) resident in HBM,
+    100,000 queries, k=10; plain and batched QPS, recall@10 and gather roofline at
+    Ls 20 / 50 / 100 / 200."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    base, graph, queries = load_c4(pgb)
+    gt_p = os.path.join(data_dir(), "c4_gt100.bin")
+    from parlayann_gpu_busqueda_b200 import formats, groundtruth
+    if os.path.exists(gt_p):
+        gt_ids, gt_d = formats.read_gt(gt_p)
+    else:
+        t = time.time()
+        gt_ids, gt_d = groundtruth.knn_gpu(base, queries, 100, local)
+        formats.write_gt(gt_p + ".tmp", gt_ids, gt_d)
+        os.replace(gt_p + ".tmp", gt_p)
+        log(f"C4 ground truth in {time.time() - t:.1f} s")
+    index = pgb.Index.flat(base, graph, device=local)
+    q = torch.from_numpy(queries).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+    peak, kind = measured_peaks()
+    gs = (int(index.info.max_degree) + 31) // 32 * 32
+    rows = []
+    for ls in C4_LS:
+        s = pgb.Searcher(index, C4_NQ, pgb.QueryParams(k=K, beam_size=ls))
+        ids = torch.empty((C4_NQ, K), dtype=torch.int32, device=dev)
+        d = torch.empty_like(ids)
+        st = torch.empty((C4_NQ, 4), dtype=torch.int32, device=dev)
+        tp = _timed_events(torch, stream, lambda: s.lanzar(q, ids, d, st, sp), args.steps,
+                           args.warmup, flush)
+        b = pgb.Batch(index, C4_NQ, max_beam=ls, max_k=K)
+        b.plan(np.full(C4_NQ, ls, np.uint32), np.full(C4_NQ, K, np.uint32))
+        bi, bd, bs = b.outputs(dev)
+        b.tune(q, bi, bd, bs)
+        b.capture(q, bi, bd, bs)
+        tb = _timed_events(torch, stream, lambda: b.replay(sp), args.steps, args.warmup, flush)
+        identical = bool(torch.equal(ids, bi) and torch.equal(d, bd))
+        stn = st.cpu().numpy()
+        rec = pgb.recall(gt_ids, gt_d, ids.cpu().numpy().view(np.uint32), K)
+        bytes_launch = float(128 * stn[:, 0].astype(np.int64).sum() + 4 * gs * stn[:, 1].astype(np.int64).sum())
+        mb = sum(tb) / len(tb) / 1e3
+        rows.append({"Ls": ls, "recall_at_10": round(rec, 5),
+                     "plain_qps": C4_NQ * len(tp) / (sum(tp) / 1e3),
+                     "batched_qps": C4_NQ / mb, "identical_neighbours": identical,
+                     "comps_per_query": float(stn[:, 0].mean()),
+                     "expansions_per_query": float(stn[:, 1].mean()),
+                     "achieved_gbs": bytes_launch / mb / 1e9,
+                     "frac": bytes_launch / mb / 1e9 / peak, "batched_config": b.config()})
+        log(rows[-1])
+        s.liberar()
+        b.close()
+    # headline row: the smallest beam at recall@10 >= 0.90
+    head = next((r for r in rows if r["recall_at_10"] >= TARGET_RECALL), rows[-1])
+    print(json.dumps({
+        "metric": "QPS at Ls 20/50/100/200, 10M uint8 d=128 Vamana, batched vs plain, 1 B200",
+        "value": head["batched_qps"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": C4_NQ / head["batched_qps"] * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint8",
+        "data": "synthetic",
+        "config": {"workload": "10M uint8 d=128 (4,096 centres, 40% zeros), Vamana R64 L128 "
+                               "alpha1.2, 100,000 queries, k=10", "headline_Ls": head["Ls"],
+                   "index_bytes": int(index.info.device_bytes),
+                   "l2": "flushed (512 MiB write) before every timed step; index 3.8 GB > L2",
+                   "rows": rows},
+        "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": head["frac"], "traffic": None, "peak_source": kind,
+                     "kernel": "flat_batched_kernel"},
+        "gpu_launches": 2 * args.steps * len(rows)}), flush=True)
 
 
 def run_mixed(args, local):
