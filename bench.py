@@ -314,20 +314,21 @@ def main():
     ap.add_argument("--profile-nq", type=int, default=8192)
     ap.add_argument("--profile-ls", type=int, default=40)
     ap.add_argument("--workload", default="vamana",
-                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving", "c4"],
+                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving", "c4", "build"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
                          "mixed: 100k queries of uneven Ls and k in one launch; serving: "
                          "Poisson bursts through the request loop; c4: 10M uint8 d=128 "
-                         "Vamana, 100k queries, Ls 20/50/100/200")
+                         "Vamana, 100k queries, Ls 20/50/100/200; build: GPU vs CPU Vamana "
+                         "construction on the 1M base")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.profile:
         run_profile(args, local)
         return
-    if args.workload in ("hnsw", "mixed", "serving", "c4") and args.impl == "ours":
-        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving,
-         "c4": run_c4}[args.workload](args, local)
+    if args.workload in ("hnsw", "mixed", "serving", "c4", "build") and args.impl == "ours":
+        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving, "c4": run_c4,
+         "build": run_build}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -604,6 +605,41 @@ def run_hnsw(args, local):
                      "frac": achieved / peak, "traffic": None, "peak_source": kind,
                      "kernel": "hnsw_kernel"},
         "gpu_launches": args.steps}), flush=True)
+
+
+def run_build(args, local):
+    """Vamana construction on the 1M int8 d=100 base (R=64, L=128, alpha=1.2, seed 0): the
+    GPU builder's wall time against the CPU builder on all host cores, and the two graphs
+    compared entry by entry."""
+    import torch
+    torch.cuda.set_device(local)
+    pgb = ge.load_package()
+    base = load_base(pgb)
+    times = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        g = pgb.build_vamana_gpu(base, R=R, L=L_BUILD, alpha=ALPHA, seed=0, device=local)
+        times.append(time.perf_counter() - t)
+    threads = os.cpu_count() or 1
+    t = time.perf_counter()
+    c = pgb.build_vamana(base, R=R, L=L_BUILD, alpha=ALPHA, seed=0)
+    t_cpu = time.perf_counter() - t
+    identical = bool(np.array_equal(g.degrees, c.degrees) and np.array_equal(g.edges, c.edges))
+    t_gpu = min(times)
+    print(json.dumps({
+        "metric": "Vamana build time, 1M int8 d=100, R=64 L=128 alpha=1.2, GPU vs CPU builder",
+        "value": t_gpu, "unit": "s", "n_gpus": 1, "steps": len(times), "warmup": 0,
+        "ms_per_step": t_gpu * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": "1M int8 d=100 Gaussian mixture, Vamana R64 L128 alpha1.2 seed 0, "
+                               "prefix-doubling batches to 2% of n", "all_runs_s": times,
+                   "identical_to_cpu_builder": identical,
+                   "mean_degree": float(g.degrees.mean()),
+                   "timing": "wall clock around the host call (upload, build, download)"},
+        "cpu_baseline": {"value": t_cpu, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": "the same full 1M build by the CPU builder"},
+        "gpu_launches": None}), flush=True)
 
 
 C4_N, C4_NQ, C4_LS = 10_000_000, 100_000, (20, 50, 100, 200)

@@ -298,6 +298,16 @@ pgb_status pgb_section_profile(uint64_t* out, uint32_t n, int reset);
 pgb_status pgb_build_vamana(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
                             uint32_t R, uint32_t L, float alpha, int passes, uint64_t seed,
                             int nthreads, uint32_t* degrees, uint32_t* adjacency);
+/* The same Vamana construction on GPU `device`. No counterpart in the reference, which
+ * searches CPU-built graphs; it is the GPU construction the reference plans
+ * (README.md:336-350: prefix-doubling batches, a search per new point, one warp per
+ * point for the prune, reverse edges through a radix sort, no atomics in the order).
+ * Identical insertion order, batches, search, prune and reverse-edge rules, so
+ * degrees/adjacency equal pgb_build_vamana's for the same arguments. Host inputs and
+ * outputs; dim <= 128. */
+pgb_status pgb_build_vamana_gpu(int device, const void* vectors, uint32_t n, uint32_t dim,
+                                pgb_elem elem, uint32_t R, uint32_t L, float alpha, int passes,
+                                uint64_t seed, uint32_t* degrees, uint32_t* adjacency);
 pgb_status pgb_build_hcnng(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
                            uint32_t trees, uint32_t leaf, uint32_t mst_deg, uint64_t seed,
                            int nthreads, uint32_t* degrees, uint32_t* adjacency);

@@ -257,6 +257,16 @@ struct DisjointSets {
 
 }  // namespace
 
+std::vector<uint32_t> vamana_insertion_order(uint32_t n, uint64_t seed) {
+    std::vector<uint32_t> order = permutation(n, seed);
+    // point 0 first: it is the entry of every search
+    auto it0 = std::find(order.begin(), order.end(), 0u);
+    std::rotate(order.begin(), it0, it0 + 1);
+    return order;
+}
+
+size_t vamana_max_batch(uint32_t n) { return std::max<size_t>(1, (size_t)(0.02 * n)); }
+
 // ---------------------------------------------------------------------------
 // Vamana (DiskANN) with prefix-doubling batch insertion. Start point 0, the point the
 // search starts from (reference busqueda.cu:166-173).
@@ -267,12 +277,9 @@ int build_vamana(const HostVectors& V, uint32_t R, uint32_t L, float alpha, int 
     std::fill(out_adj, out_adj + (size_t)n * R, kNoNeighbor);
     std::fill(out_deg, out_deg + n, 0u);
     if (n <= 1) return 0;
-    std::vector<uint32_t> order = permutation(n, seed);
-    // point 0 first: it is the entry of every search
-    auto it0 = std::find(order.begin(), order.end(), 0u);
-    std::rotate(order.begin(), it0, it0 + 1);
+    const std::vector<uint32_t> order = vamana_insertion_order(n, seed);
     const std::vector<uint32_t> starts{0};
-    const size_t max_batch = std::max<size_t>(1, (size_t)(0.02 * n));
+    const size_t max_batch = vamana_max_batch(n);
     for (int pass = 0; pass < passes; pass++) {
         const float a = (passes > 1 && pass == 0) ? 1.0f : alpha;
         size_t pos = (pass == 0) ? 1 : 0;

@@ -21,6 +21,11 @@ struct HnswBuilt {
 
 int build_vamana(const HostVectors& V, uint32_t R, uint32_t L, float alpha, int passes,
                  uint64_t seed, int nthreads, uint32_t* out_deg, uint32_t* out_adj);
+// Vamana's insertion schedule, shared by the CPU and GPU builders: a seeded permutation
+// with point 0 moved to the front, inserted in prefix-doubling batches 1, 2, 4, ... up
+// to vamana_max_batch(n) points (2 % of n) per batch
+std::vector<uint32_t> vamana_insertion_order(uint32_t n, uint64_t seed);
+size_t vamana_max_batch(uint32_t n);
 int build_hcnng(const HostVectors& V, uint32_t trees, uint32_t leaf, uint32_t mst_deg,
                 uint64_t seed, int nthreads, uint32_t* out_deg, uint32_t* out_adj);
 int build_nndescent(const HostVectors& V, uint32_t K, uint32_t init_trees, uint32_t leaf,

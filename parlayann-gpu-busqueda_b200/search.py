@@ -189,6 +189,17 @@ def build_vamana(x: np.ndarray, R: int = 32, L: int = 64, alpha: float = 1.2, pa
     return Graph.from_padded(deg, adj)
 
 
+def build_vamana_gpu(x: np.ndarray, R: int = 32, L: int = 64, alpha: float = 1.2,
+                     passes: int = 1, seed: int = 0, device: int = 0) -> Graph:
+    """build_vamana on the GPU: the same graph for the same arguments."""
+    x = np.ascontiguousarray(x)
+    deg = np.empty(x.shape[0], dtype=np.uint32)
+    adj = np.empty((x.shape[0], R), dtype=np.uint32)
+    N.check(N.lib.pgb_build_vamana_gpu(device, _ptr(x), x.shape[0], x.shape[1], _elem(x.dtype),
+                                       R, L, alpha, passes, seed, _ptr(deg), _ptr(adj)))
+    return Graph.from_padded(deg, adj)
+
+
 def build_hcnng(x: np.ndarray, trees: int = 30, leaf: int = 1000, mst_deg: int = 3,
                 seed: int = 0, threads: int = 0) -> Graph:
     x = np.ascontiguousarray(x)

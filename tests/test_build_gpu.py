@@ -1,0 +1,75 @@
+"""GPU Vamana construction (pgb_build_vamana_gpu) against the CPU builder: the same
+insertion order, batches, search, prune and reverse-edge rules, so the graphs must be
+identical -- degrees and every row, in order."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+def both(pgb, x, **kw):
+    cpu = pgb.build_vamana(x, **kw)
+    gpu = pgb.build_vamana_gpu(x, **kw)
+    return cpu, gpu
+
+
+def assert_same_graph(tag, a, b):
+    assert_same(f"{tag} degrees", b.degrees, a.degrees)
+    assert_same(f"{tag} edges", b.edges, a.edges)
+
+
+@pytest.mark.parametrize("R,L,alpha", [(32, 64, 1.2), (16, 40, 1.0), (64, 100, 1.2)])
+def test_gpu_vamana_equals_cpu_int8(pgb, golden, gpu, R, L, alpha):
+    cpu, g = both(pgb, golden.base, R=R, L=L, alpha=alpha, seed=0)
+    assert_same_graph(f"R{R} L{L} a{alpha}", cpu, g)
+
+
+def test_gpu_vamana_equals_cpu_uint8_d128(pgb, gpu):
+    from parlayann_gpu_busqueda_b200.synthetic import LAW_C4
+    x = LAW_C4.sample(3000, 3, 0)
+    cpu, g = both(pgb, x, R=24, L=48, alpha=1.2, seed=5)
+    assert_same_graph("uint8", cpu, g)
+
+
+def test_gpu_vamana_two_passes_and_ties(pgb, golden, gpu):
+    cpu, g = both(pgb, golden.base, R=24, L=48, alpha=1.2, passes=2, seed=1)
+    assert_same_graph("2 passes", cpu, g)
+    # duplicate vectors and equal distances everywhere
+    cpu, g = both(pgb, golden.ties_base, R=16, L=32, alpha=1.2, seed=0)
+    assert_same_graph("ties", cpu, g)
+
+
+def test_gpu_vamana_retries_and_hubs_give_the_same_graph(pgb, golden, gpu):
+    """Tiny first tables: most searches outgrow them and run again with larger ones, and
+    most reverse-edge merges take the second (hub) launch; the graph must not change."""
+    os.environ["PGB_BUILD_SMALL_TABLES"] = "1"
+    try:
+        g = pgb.build_vamana_gpu(golden.base, R=32, L=64, alpha=1.2, seed=0)
+    finally:
+        del os.environ["PGB_BUILD_SMALL_TABLES"]
+    cpu = pgb.build_vamana(golden.base, R=32, L=64, alpha=1.2, seed=0)
+    assert_same_graph("small tables", cpu, g)
+
+
+def test_gpu_vamana_graph_searches_like_cpu_graph(pgb, oracle, golden, gpu):
+    """The built graph is a working index: GPU search on it equals the oracle's."""
+    g = pgb.build_vamana_gpu(golden.base, R=32, L=64, alpha=1.2, seed=0)
+    index = pgb.Index.flat(golden.base, g)
+    s = pgb.Searcher(index, len(golden.queries), pgb.QueryParams(k=10, beam_size=40))
+    ids, dists, _ = s.search(golden.queries)
+    s.liberar()
+    index.close()
+    oid, od, *_ = oracle.flat_search(golden.base, g.degrees, g.edges, golden.queries, 10, 40)
+    assert_same("ids", ids, oid)
+    assert_same("dists", dists, od)
+
+
+def test_gpu_vamana_rejects_bad_arguments(pgb, golden, gpu):
+    with pytest.raises(pgb.PgbError):
+        pgb.build_vamana_gpu(golden.base, R=0, L=64)
+    with pytest.raises(pgb.PgbError):
+        pgb.build_vamana_gpu(np.zeros((10, 129), np.int8), R=8, L=16)
