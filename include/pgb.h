@@ -319,6 +319,13 @@ pgb_status pgb_build_nndescent(const void* vectors, uint32_t n, uint32_t dim, pg
 pgb_status pgb_build_hnsw(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
                           uint32_t M, uint32_t ef_construction, float ml, float alpha,
                           uint64_t seed, int nthreads, const char* path);
+/* The same HNSW construction on GPU `device` (no counterpart in the reference; the HNSW
+ * step of its planned GPU construction, README.md:350): identical levels, insertion
+ * batches, descent, per-level search, selection and reverse-edge rules, so the file is
+ * byte-identical to pgb_build_hnsw's for the same arguments. dim <= 128. */
+pgb_status pgb_build_hnsw_gpu(int device, const void* vectors, uint32_t n, uint32_t dim,
+                              pgb_elem elem, uint32_t M, uint32_t ef_construction, float ml,
+                              float alpha, uint64_t seed, const char* path);
 /* ParlayANN graph file from a padded adjacency (row i: degrees[i] ids, stride slots). */
 pgb_status pgb_write_graph(const char* path, uint32_t n, uint32_t slots,
                            const uint32_t* degrees, const uint32_t* adjacency);

@@ -501,18 +501,27 @@ static void hnsw_select(const HostVectors& V, uint32_t p, std::vector<DistId>& c
     }
 }
 
+std::vector<uint32_t> hnsw_levels(uint32_t n, float ml, uint64_t seed) {
+    std::vector<uint32_t> level(n, 0);
+    SplitMix64 rng(seed);
+    for (uint32_t i = 0; i < n; i++) {
+        double u = rng.uniform();
+        if (u <= 0) u = 1e-300;
+        level[i] = (uint32_t)std::min(30.0, std::floor(-std::log(u) * ml));
+    }
+    return level;
+}
+
+std::vector<uint32_t> hnsw_insertion_order(uint32_t n, uint64_t seed) {
+    return permutation(n, seed ^ 0x5bd1e995ull);
+}
+
 int build_hnsw(const HostVectors& V, uint32_t M, uint32_t efc, float ml, float alpha,
                uint64_t seed, int nthreads, HnswBuilt& H) {
     const uint32_t n = V.n;
     H.n = n;
     H.M = M;
-    H.level.assign(n, 0);
-    SplitMix64 rng(seed);
-    for (uint32_t i = 0; i < n; i++) {
-        double u = rng.uniform();
-        if (u <= 0) u = 1e-300;
-        H.level[i] = (uint32_t)std::min(30.0, std::floor(-std::log(u) * ml));
-    }
+    H.level = hnsw_levels(n, ml, seed);
     auto cap = [&](uint32_t l) { return l == 0 ? 2 * M : M; };
     H.first.resize(n);
     H.row_off.clear();
@@ -530,7 +539,7 @@ int build_hnsw(const HostVectors& V, uint32_t M, uint32_t efc, float ml, float a
     auto row = [&](uint32_t i, uint32_t l) { return H.rows.data() + H.row_off[H.first[i] + l]; };
     auto size = [&](uint32_t i, uint32_t l) -> uint32_t& { return H.sizes[H.first[i] + l]; };
 
-    std::vector<uint32_t> order = permutation(n, seed ^ 0x5bd1e995ull);
+    std::vector<uint32_t> order = hnsw_insertion_order(n, seed);
     uint32_t top = 0;
     H.entry = order[0];
     top = H.level[H.entry];

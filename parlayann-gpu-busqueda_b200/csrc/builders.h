@@ -33,5 +33,9 @@ int build_nndescent(const HostVectors& V, uint32_t K, uint32_t init_trees, uint3
                     uint32_t* out_deg, uint32_t* out_adj);
 int build_hnsw(const HostVectors& V, uint32_t M, uint32_t efc, float ml, float alpha,
                uint64_t seed, int nthreads, HnswBuilt& H);
+// HNSW's node levels (floor(-ln(U) * ml), at most 30) and insertion order, shared by the
+// CPU and GPU builders; insertion runs in the same prefix-doubling batches as Vamana's
+std::vector<uint32_t> hnsw_levels(uint32_t n, float ml, uint64_t seed);
+std::vector<uint32_t> hnsw_insertion_order(uint32_t n, uint64_t seed);
 
 }  // namespace pgb

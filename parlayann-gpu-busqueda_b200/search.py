@@ -230,6 +230,14 @@ def build_hnsw(x: np.ndarray, path: str, M: int = 32, ef_construction: int = 128
                                  ef_construction, ml, alpha, seed, threads, path.encode()))
 
 
+def build_hnsw_gpu(x: np.ndarray, path: str, M: int = 32, ef_construction: int = 128,
+                   ml: float = 0.36, alpha: float = 0.83, seed: int = 0, device: int = 0) -> None:
+    """build_hnsw on the GPU: the same file for the same arguments."""
+    x = np.ascontiguousarray(x)
+    N.check(N.lib.pgb_build_hnsw_gpu(device, _ptr(x), x.shape[0], x.shape[1], _elem(x.dtype), M,
+                                     ef_construction, ml, alpha, seed, path.encode()))
+
+
 def file_check(path: str, kind: str):
     """C-reader validation of a file on the host: kind 'vectors', 'graph' or 'hnsw'.
     Returns the 4 info counters; raises PgbError (IO or FORMAT) on a bad file."""

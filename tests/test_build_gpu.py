@@ -68,6 +68,48 @@ def test_gpu_vamana_graph_searches_like_cpu_graph(pgb, oracle, golden, gpu):
     assert_same("dists", dists, od)
 
 
+def hnsw_files(pgb, tmp_path, x, **kw):
+    cpu_p, gpu_p = str(tmp_path / "cpu.hnsw"), str(tmp_path / "gpu.hnsw")
+    pgb.build_hnsw(x, cpu_p, **kw)
+    pgb.build_hnsw_gpu(x, gpu_p, **kw)
+    return open(cpu_p, "rb").read(), open(gpu_p, "rb").read(), gpu_p
+
+
+@pytest.mark.parametrize("M,efc,ml", [(16, 64, 0.36), (8, 32, 0.6)])
+def test_gpu_hnsw_file_equals_cpu_int8(pgb, golden, gpu, tmp_path, M, efc, ml):
+    cpu, g, _ = hnsw_files(pgb, tmp_path, golden.base, M=M, ef_construction=efc, ml=ml, alpha=0.83)
+    assert g == cpu, "GPU HNSW file differs from the CPU builder's"
+
+
+def test_gpu_hnsw_file_equals_cpu_uint8_and_ties(pgb, golden, gpu, tmp_path):
+    from parlayann_gpu_busqueda_b200.synthetic import LAW_C4
+    x = LAW_C4.sample(2500, 4, 0)
+    cpu, g, _ = hnsw_files(pgb, tmp_path, x, M=12, ef_construction=40, ml=0.5, alpha=1.0, seed=3)
+    assert g == cpu, "uint8"
+    cpu, g, _ = hnsw_files(pgb, tmp_path, golden.ties_base, M=8, ef_construction=32, ml=0.5)
+    assert g == cpu, "ties"
+
+
+def test_gpu_hnsw_small_tables_and_search(pgb, oracle, golden, gpu, tmp_path):
+    """Tiny first tables (retried searches, hub merges) give the same file, and the model
+    searches like the oracle says."""
+    os.environ["PGB_BUILD_SMALL_TABLES"] = "1"
+    try:
+        cpu, g, gpu_p = hnsw_files(pgb, tmp_path, golden.base, M=16, ef_construction=64, ml=0.36)
+    finally:
+        del os.environ["PGB_BUILD_SMALL_TABLES"]
+    assert g == cpu
+    h = pgb.read_hnsw(gpu_p)
+    index = pgb.Index.hnsw(golden.base, h)
+    s = pgb.Searcher(index, len(golden.queries), pgb.QueryParams(k=10, beam_size=50))
+    ids, dists, _ = s.search(golden.queries)
+    s.liberar()
+    index.close()
+    oid, od, *_ = oracle.hnsw_search(golden.base, h, golden.queries, 10, 50)
+    assert_same("ids", ids, oid)
+    assert_same("dists", dists, od)
+
+
 def test_gpu_vamana_rejects_bad_arguments(pgb, golden, gpu):
     with pytest.raises(pgb.PgbError):
         pgb.build_vamana_gpu(golden.base, R=0, L=64)
