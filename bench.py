@@ -126,10 +126,11 @@ def load_hnsw(pgb):
     p = os.path.join(data_dir(), HNSW_FILE)
     base = load_base(pgb)
     if not os.path.exists(p):
+        # the GPU builder writes the CPU builder's file (tests/test_build_gpu.py)
         t = time.time()
-        pgb.build_hnsw(base, p + ".tmp", M=32, ef_construction=128, ml=0.36, alpha=0.83, seed=0)
+        pgb.build_hnsw_gpu(base, p + ".tmp", M=32, ef_construction=128, ml=0.36, alpha=0.83, seed=0)
         os.replace(p + ".tmp", p)
-        log(f"built HNSW 1M in {time.time() - t:.1f} s")
+        log(f"built HNSW 1M on the GPU in {time.time() - t:.1f} s")
     return base, pgb.read_hnsw(p)
 
 
@@ -628,6 +629,20 @@ def run_build(args, local):
     t_cpu = time.perf_counter() - t
     identical = bool(np.array_equal(g.degrees, c.degrees) and np.array_equal(g.edges, c.edges))
     t_gpu = min(times)
+    # HNSW M=32 efC=128 on the same base: GPU and CPU model files compared byte for byte
+    hp_gpu = os.path.join(data_dir(), "build_gpu.hnsw")
+    hp_cpu = os.path.join(data_dir(), "build_cpu.hnsw")
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    pgb.build_hnsw_gpu(base, hp_gpu, M=32, ef_construction=128, ml=0.36, alpha=0.83, seed=0, device=local)
+    h_gpu = time.perf_counter() - t
+    t = time.perf_counter()
+    pgb.build_hnsw(base, hp_cpu, M=32, ef_construction=128, ml=0.36, alpha=0.83, seed=0)
+    h_cpu = time.perf_counter() - t
+    with open(hp_gpu, "rb") as fa, open(hp_cpu, "rb") as fb:
+        h_same = fa.read() == fb.read()
+    for p in (hp_gpu, hp_cpu):
+        os.unlink(p)
     print(json.dumps({
         "metric": "Vamana build time, 1M int8 d=100, R=64 L=128 alpha=1.2, GPU vs CPU builder",
         "value": t_gpu, "unit": "s", "n_gpus": 1, "steps": len(times), "warmup": 0,
@@ -637,6 +652,8 @@ def run_build(args, local):
                                "prefix-doubling batches to 2% of n", "all_runs_s": times,
                    "identical_to_cpu_builder": identical,
                    "mean_degree": float(g.degrees.mean()),
+                   "hnsw_M32_efc128": {"gpu_s": h_gpu, "cpu_s": h_cpu, "cpu_cores": os.cpu_count(),
+                                       "file_identical_to_cpu_builder": bool(h_same)},
                    "timing": "wall clock around the host call (upload, build, download)"},
         "cpu_baseline": {"value": t_cpu, "unit": "s", "cores": threads, "kind": "port",
                          "sample": "the same full 1M build by the CPU builder"},
