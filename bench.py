@@ -643,6 +643,15 @@ def run_build(args, local):
         h_same = fa.read() == fb.read()
     for p in (hp_gpu, hp_cpu):
         os.unlink(p)
+    # HCNNG 30 trees, leaves of 1,000, MST degree 3
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    hg = pgb.build_hcnng_gpu(base, trees=30, leaf=1000, mst_deg=3, seed=0, device=local)
+    c_gpu = time.perf_counter() - t
+    t = time.perf_counter()
+    hc = pgb.build_hcnng(base, trees=30, leaf=1000, mst_deg=3, seed=0)
+    c_cpu = time.perf_counter() - t
+    c_same = bool(np.array_equal(hg.degrees, hc.degrees) and np.array_equal(hg.edges, hc.edges))
     print(json.dumps({
         "metric": "Vamana build time, 1M int8 d=100, R=64 L=128 alpha=1.2, GPU vs CPU builder",
         "value": t_gpu, "unit": "s", "n_gpus": 1, "steps": len(times), "warmup": 0,
@@ -654,6 +663,9 @@ def run_build(args, local):
                    "mean_degree": float(g.degrees.mean()),
                    "hnsw_M32_efc128": {"gpu_s": h_gpu, "cpu_s": h_cpu, "cpu_cores": os.cpu_count(),
                                        "file_identical_to_cpu_builder": bool(h_same)},
+                   "hcnng_T30_leaf1000_mst3": {"gpu_s": c_gpu, "cpu_s": c_cpu, "cpu_cores": os.cpu_count(),
+                                               "identical_to_cpu_builder": c_same,
+                                               "mean_degree": float(hg.degrees.mean())},
                    "timing": "wall clock around the host call (upload, build, download)"},
         "cpu_baseline": {"value": t_cpu, "unit": "s", "cores": threads, "kind": "port",
                          "sample": "the same full 1M build by the CPU builder"},

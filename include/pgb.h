@@ -311,6 +311,14 @@ pgb_status pgb_build_vamana_gpu(int device, const void* vectors, uint32_t n, uin
 pgb_status pgb_build_hcnng(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
                            uint32_t trees, uint32_t leaf, uint32_t mst_deg, uint64_t seed,
                            int nthreads, uint32_t* degrees, uint32_t* adjacency);
+/* The same HCNNG construction on GPU `device` (no counterpart in the reference; the HCNNG
+ * step of its planned GPU construction, README.md:351-353: exact 10-NN inside each
+ * cluster-tree leaf, a degree-bounded MST per leaf, one warp per leaf). Identical trees,
+ * leaf neighbours, MST order and row order, so degrees/adjacency equal pgb_build_hcnng's
+ * for the same arguments. dim <= 128, leaf <= 1024, n < 2^31. */
+pgb_status pgb_build_hcnng_gpu(int device, const void* vectors, uint32_t n, uint32_t dim,
+                               pgb_elem elem, uint32_t trees, uint32_t leaf, uint32_t mst_deg,
+                               uint64_t seed, uint32_t* degrees, uint32_t* adjacency);
 pgb_status pgb_build_nndescent(const void* vectors, uint32_t n, uint32_t dim, pgb_elem elem,
                                uint32_t K, uint32_t init_trees, uint32_t leaf, float alpha,
                                float delta, uint32_t max_iters, uint64_t seed, int nthreads,

@@ -91,6 +91,8 @@ _sig("pgb_build_vamana_gpu", C.c_int, C.c_int, vp, u32, u32, C.c_int, u32, u32, 
 _sig("pgb_build_hnsw_gpu", C.c_int, C.c_int, vp, u32, u32, C.c_int, u32, u32, C.c_float,
      C.c_float, u64, C.c_char_p)
 _sig("pgb_build_hcnng", C.c_int, vp, u32, u32, C.c_int, u32, u32, u32, u64, C.c_int, vp, vp)
+_sig("pgb_build_hcnng_gpu", C.c_int, C.c_int, vp, u32, u32, C.c_int, u32, u32, u32, u64, vp,
+     vp)
 _sig("pgb_build_nndescent", C.c_int, vp, u32, u32, C.c_int, u32, u32, u32, C.c_float,
      C.c_float, u32, u64, C.c_int, vp, vp)
 _sig("pgb_build_hnsw", C.c_int, vp, u32, u32, C.c_int, u32, u32, C.c_float, C.c_float, u64,

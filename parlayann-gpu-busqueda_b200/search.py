@@ -211,6 +211,18 @@ def build_hcnng(x: np.ndarray, trees: int = 30, leaf: int = 1000, mst_deg: int =
     return Graph.from_padded(deg, adj)
 
 
+def build_hcnng_gpu(x: np.ndarray, trees: int = 30, leaf: int = 1000, mst_deg: int = 3,
+                    seed: int = 0, device: int = 0) -> Graph:
+    """build_hcnng on the GPU: the same graph for the same arguments (leaf <= 1024)."""
+    x = np.ascontiguousarray(x)
+    slots = trees * mst_deg
+    deg = np.empty(x.shape[0], dtype=np.uint32)
+    adj = np.empty((x.shape[0], slots), dtype=np.uint32)
+    N.check(N.lib.pgb_build_hcnng_gpu(device, _ptr(x), x.shape[0], x.shape[1], _elem(x.dtype),
+                                      trees, leaf, mst_deg, seed, _ptr(deg), _ptr(adj)))
+    return Graph.from_padded(deg, adj)
+
+
 def build_nndescent(x: np.ndarray, K: int = 40, init_trees: int = 10, leaf: int = 1000,
                     alpha: float = 1.2, delta: float = 0.05, max_iters: int = 8, seed: int = 0,
                     threads: int = 0) -> Graph:

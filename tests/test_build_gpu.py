@@ -1,6 +1,8 @@
-"""GPU Vamana construction (pgb_build_vamana_gpu) against the CPU builder: the same
-insertion order, batches, search, prune and reverse-edge rules, so the graphs must be
-identical -- degrees and every row, in order."""
+"""GPU graph construction against the CPU builders: Vamana (pgb_build_vamana_gpu: the same
+insertion order, batches, search, prune and reverse-edge rules), HNSW (pgb_build_hnsw_gpu:
+byte-identical model files) and HCNNG (pgb_build_hcnng_gpu: the same trees, leaf
+neighbours and MST order). The graphs must be identical -- degrees and every row, in
+order."""
 import os
 
 import numpy as np
@@ -108,6 +110,43 @@ def test_gpu_hnsw_small_tables_and_search(pgb, oracle, golden, gpu, tmp_path):
     oid, od, *_ = oracle.hnsw_search(golden.base, h, golden.queries, 10, 50)
     assert_same("ids", ids, oid)
     assert_same("dists", dists, od)
+
+
+def test_gpu_hcnng_reproduces_the_golden_graph(pgb, golden, gpu):
+    """c1s_hcnng.graph was written by the CPU builder with these arguments."""
+    g = pgb.build_hcnng_gpu(golden.base, trees=10, leaf=400, mst_deg=3, seed=0)
+    assert_same_graph("golden", golden.graphs["hcnng"], g)
+
+
+@pytest.mark.parametrize("trees,leaf,mst_deg,seed", [(6, 300, 3, 3), (4, 1024, 2, 1), (3, 11, 4, 2),
+                                                     (2, 2, 3, 5), (5, 64, 1, 0)])
+def test_gpu_hcnng_equals_cpu_int8(pgb, golden, gpu, trees, leaf, mst_deg, seed):
+    """Leaves of up to 1,024 points; of at most 11 (fewer than 10 neighbours each); of at
+    most 2 (halved ranges everywhere); single-edge MST degree."""
+    kw = dict(trees=trees, leaf=leaf, mst_deg=mst_deg, seed=seed)
+    cpu = pgb.build_hcnng(golden.base, **kw)
+    g = pgb.build_hcnng_gpu(golden.base, **kw)
+    assert_same_graph(f"T{trees} leaf{leaf} mst{mst_deg}", cpu, g)
+
+
+def test_gpu_hcnng_equals_cpu_uint8_d128_and_ties(pgb, golden, gpu):
+    from parlayann_gpu_busqueda_b200.synthetic import LAW_C4
+    x = LAW_C4.sample(3000, 3, 0)
+    kw = dict(trees=5, leaf=700, mst_deg=3, seed=4)
+    assert_same_graph("uint8", pgb.build_hcnng(x, **kw), pgb.build_hcnng_gpu(x, **kw))
+    # every vector three times: equal distances everywhere
+    kw = dict(trees=4, leaf=100, mst_deg=3, seed=0)
+    assert_same_graph("ties", pgb.build_hcnng(golden.ties_base, **kw),
+                      pgb.build_hcnng_gpu(golden.ties_base, **kw))
+
+
+def test_gpu_hcnng_rejects_bad_arguments(pgb, golden, gpu):
+    with pytest.raises(pgb.PgbError, match="1,024"):
+        pgb.build_hcnng_gpu(golden.base, trees=2, leaf=1025)
+    with pytest.raises(pgb.PgbError):
+        pgb.build_hcnng_gpu(golden.base, trees=100, mst_deg=3)  # 300 slots > 256
+    with pytest.raises(pgb.PgbError):
+        pgb.build_hcnng_gpu(golden.base, trees=2, leaf=1)
 
 
 def test_gpu_vamana_rejects_bad_arguments(pgb, golden, gpu):
