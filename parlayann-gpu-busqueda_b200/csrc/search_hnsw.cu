@@ -114,6 +114,7 @@ struct HnswArgs {
     uint32_t* inw;
     unsigned long long* gfilter;
     uint64_t epoch_base;
+    uint32_t* queue;  // query work queue: each warp takes the next query when it is free
 };
 
 // is_inw is an exact set private to the search (only membership matters, not where ids
@@ -185,7 +186,6 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     const int w = threadIdx.x >> 5;
     const uint32_t wpb = blockDim.x >> 5;
     const uint32_t gw = blockIdx.x * wpb + w;
-    const uint32_t total = gridDim.x * wpb;
     const HnswLayout& L = A.L;
     unsigned char* wmem = smem + (size_t)w * L.bytes;
     uint32_t* qwords = reinterpret_cast<uint32_t*>(wmem);
@@ -211,8 +211,15 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     const int ccap = (int)hnsw_ccap(L.wcap);
     const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
     const uint32_t layers = A.top + 1u;
+    // queries are taken from the work queue, so a warp that drew short searches takes more
+    // of them and the launch does not wait on the warps with the longest share
+    auto take = [&]() -> uint32_t {
+        uint32_t v = 0;
+        if (lane == 0) v = atomicAdd(A.queue, 1u);
+        return __shfl_sync(kFull, v, 0);
+    };
 
-    for (uint32_t q = gw; q < A.nq; q += total) {
+    for (uint32_t q = take(); q < A.nq; q = take()) {
         load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
         __syncwarp();
         const int4* q4 = reinterpret_cast<const int4*>(qwords);
@@ -371,6 +378,14 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     }
                     uint32_t* sslot = reinterpret_cast<uint32_t*>(akey);
                     uint32_t* sid = sslot + 32 * CH;
+                    // slots of this row's earlier chunks, hashed into 2,048 bits (in nkey,
+                    // unused until the cand update): a clear bit proves that no earlier
+                    // chunk wrote the slot, so the backward scan runs only on a set bit
+                    uint32_t* rbits = reinterpret_cast<uint32_t*>(nkey);
+                    if (CH > 1) {
+                        reinterpret_cast<uint2*>(rbits)[lane] = make_uint2(0u, 0u);
+                        __syncwarp();
+                    }
 #pragma unroll
                     for (int t = 0; t < CH; t++) {
                         const uint32_t x = a[t];
@@ -379,12 +394,13 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         const uint32_t before = peers & lt;
                         const int src = before ? 31 - __clz(before) : lane;
                         const uint32_t prev = __shfl_sync(kFull, x, src);
+                        const uint32_t rb = slot[t] & 2047u;
                         bool seen;
                         if (before) {
                             seen = part && prev == x;
                         } else {
                             seen = part && mem[t] == x;
-                            if (part)
+                            if (t > 0 && part && ((rbits[rb >> 5] >> (rb & 31u)) & 1u))
                                 for (int p = t * 32 - 1; p >= 0; p--)
                                     if (sslot[p] == slot[t]) {
                                         seen = sid[p] == x;
@@ -394,6 +410,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         __syncwarp();
                         sslot[t * 32 + lane] = slot[t];
                         sid[t * 32 + lane] = x;
+                        if (CH > 1 && t + 1 < CH && part && (peers & gt) == 0)
+                            atomicOr(&rbits[rb >> 5], 1u << (rb & 31u));
                         if (part && (peers & gt) == 0) {
                             if (FMODE == 1) {
                                 gf32[slot[t]] = x;
@@ -700,6 +718,7 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     // needs no clearing
     const size_t inw_bytes = 4ull * H.cap_inw * H.total_warps;
     if ((s = hnsw_cuda(cudaMalloc(&H.inw, inw_bytes), "is_inw tables")) != PGB_OK) return s;
+    if ((s = hnsw_cuda(cudaMalloc(&H.queue, sizeof(uint32_t)), "query queue")) != PGB_OK) return s;
     if (H.fmode == 1) {  // ids only; validity is the shared written-slot bitmap
         if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, 4ull * H.filter_slots * H.total_warps),
                            "filter tables")) != PGB_OK)
@@ -762,6 +781,11 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     }
     A.epoch_base = H.epoch_base;
     H.epoch_base += need;
+    A.queue = H.queue;
+    {
+        const pgb_status s = hnsw_cuda(cudaMemsetAsync(H.queue, 0, sizeof(uint32_t), stream), "query queue");
+        if (s != PGB_OK) return s;
+    }
     void* args[] = {&A};
     cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
                                      H.smem_bytes, stream);
@@ -771,6 +795,7 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
 void hnsw_release(HnswState& H) {
     cudaFree(H.inw);
     cudaFree(H.gfilter);
+    cudaFree(H.queue);
     H = HnswState{};
 }
 

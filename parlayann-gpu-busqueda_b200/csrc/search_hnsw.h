@@ -28,6 +28,7 @@ struct HnswState {
     unsigned long long* gfilter = nullptr; // global lossy filter per warp: 4-byte ids
                                            // (fmode 1) or (epoch, id) pairs (fmode 2)
     uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
+    uint32_t* queue = nullptr;             // next query of the running launch (zeroed per launch)
 };
 
 pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswState& H);
