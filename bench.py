@@ -253,6 +253,62 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def section_shares(pgb, run, steps):
+    """Section cycle shares and event counts per expansion of `steps` calls of run() under
+    the profiling library (None under the plain library)."""
+    if not os.environ.get("PGB_LIB", "").endswith("libpgb_prof.so"):
+        return None
+    import ctypes
+    names = pgb._native.SECTION_NAMES
+    nt = pgb._native.N_TIMED_SECTIONS
+    buf = (ctypes.c_uint64 * len(names))()
+    pgb._native.check(pgb._native.lib.pgb_section_profile(buf, len(names), 1))
+    for _ in range(steps):
+        run()
+    pgb._native.check(pgb._native.lib.pgb_section_profile(buf, len(names), 1))
+    cyc = list(buf)[:nt]
+    tot = sum(cyc)
+    sections = {n: round(c / tot, 4) for n, c in zip(names, cyc)}
+    n_exp = max(1, buf[nt])
+    sections["cycles_per_expansion"] = tot / n_exp
+    for n, c in zip(names[nt + 2:], list(buf)[nt + 2:]):
+        sections[n + "_per_expansion"] = round(c / n_exp, 3)
+    return sections
+
+
+def run_profile_hnsw(args, local):
+    """Launches only the HNSW search kernel (M=32 model of the 1M base) on a small query set;
+    under the profiling library, its section shares (filter / distances / acceptance = sort /
+    cand update = union / W update = shift)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    from parlayann_gpu_busqueda_b200.synthetic import LAW_C2
+    base, h = load_hnsw(pgb)
+    nq, Ls = args.profile_nq, args.profile_ls
+    queries = LAW_C2.sample(nq, 0, 1)
+    index = pgb.Index.hnsw(base, h, device=local)
+    q = torch.from_numpy(np.ascontiguousarray(queries).view(np.uint8)).to(dev)
+    sp = torch.cuda.current_stream(dev).cuda_stream
+    s = pgb.Searcher(index, nq, pgb.QueryParams(k=K, beam_size=Ls))
+    ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
+    d = torch.empty_like(ids)
+    st = torch.empty((nq, 4), dtype=torch.int32, device=dev)
+    for _ in range(args.warmup + args.steps):
+        s.lanzar(q, ids, d, st, sp)
+    torch.cuda.synchronize(dev)
+
+    def run():
+        s.lanzar(q, ids, d, st, sp)
+        torch.cuda.synchronize(dev)
+    sections = section_shares(pgb, run, args.steps)
+    stn = st.cpu().numpy()
+    print(json.dumps({"profile": "hnsw", "nq": nq, "Ls": Ls, "sections": sections,
+                      "comps": int(stn[:, 0].astype(np.int64).sum()),
+                      "expansions": int(stn[:, 1].astype(np.int64).sum())}))
+
+
 def run_profile(args, local):
     """Launches only the search kernels (plain, then batched) on a small query set."""
     import torch
@@ -277,26 +333,12 @@ def run_profile(args, local):
         b.search(q, ids, d, st, sp)
     torch.cuda.synchronize(dev)
     stn = st.cpu().numpy()
-    sections = None
-    if os.environ.get("PGB_LIB", "").endswith("libpgb_prof.so"):
-        # section cycles of the batched launches only: reset, run, read
-        import ctypes
-        names = pgb._native.SECTION_NAMES
-        nt = pgb._native.N_TIMED_SECTIONS
-        buf = (ctypes.c_uint64 * len(names))()
-        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, len(names), 1))
-        for _ in range(args.steps):
-            b.search(q, ids, d, st, sp)
+
+    # section cycles of the batched launches only
+    def run():
+        b.search(q, ids, d, st, sp)
         torch.cuda.synchronize(dev)
-        pgb._native.check(pgb._native.lib.pgb_section_profile(buf, len(names), 1))
-        cyc = list(buf)[:nt]
-        tot = sum(cyc)
-        sections = {n: round(c / tot, 4) for n, c in zip(names, cyc)}
-        n_exp = max(1, buf[nt])
-        sections["cycles_per_expansion"] = tot / n_exp
-        # event counts per expansion
-        for n, c in zip(names[nt + 2:], list(buf)[nt + 2:]):
-            sections[n + "_per_expansion"] = round(c / n_exp, 3)
+    sections = section_shares(pgb, run, args.steps)
     print(json.dumps({"profile": True, "nq": nq, "Ls": Ls, "sections": sections,
                       "comps": int(stn[:, 0].astype(np.int64).sum()),
                       "expansions": int(stn[:, 1].astype(np.int64).sum()),
@@ -326,7 +368,10 @@ def main():
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.profile:
-        run_profile(args, local)
+        if args.workload == "hnsw":
+            run_profile_hnsw(args, local)
+        else:
+            run_profile(args, local)
         return
     if args.workload in ("hnsw", "mixed", "serving", "c4", "build") and args.impl == "ours":
         {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving, "c4": run_c4,

@@ -6,6 +6,7 @@
 
 #include "errors.h"
 #include "search_flat.cuh"
+#include "search_hnsw.h"
 #include "search_plan.h"
 
 namespace pgb {
@@ -137,6 +138,7 @@ extern "C" pgb_status pgb_section_profile(uint64_t* out, uint32_t n, int reset) 
     if (e == cudaSuccess) e = pgb::flat_section_totals_ch3(acc, reset != 0);
     if (e == cudaSuccess) e = pgb::flat_section_totals_ch4(acc, reset != 0);
     if (e == cudaSuccess) e = pgb::flat_section_totals_ch8(acc, reset != 0);
+    if (e == cudaSuccess) e = pgb::hnsw_section_totals(acc, reset != 0);
     if (e != cudaSuccess) return pgb::fail(PGB_ERR_CUDA, cudaGetErrorString(e));
     for (int i = 0; i < pgb::NUM_SECTIONS; i++) out[i] = acc[i];
     return PGB_OK;

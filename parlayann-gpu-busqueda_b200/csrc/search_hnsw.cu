@@ -39,7 +39,7 @@ __host__ __device__ inline uint32_t hnsw_cap_inw(uint32_t Ls) {
 struct HnswLayout {
     uint32_t wcap, gs, filter_words, cap_inw, wbits_words;
     uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_ibits,
-        off_occ, off_wbits, off_filter, bytes;
+        off_occ, off_wbits, off_filter, off_prof, bytes;
 };
 
 // "maybe in is_inw" bitmap per warp: a clear bit proves absence, so most membership
@@ -88,6 +88,8 @@ __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t g
     o = round16(o + 4u * wbits_words);
     L.off_filter = o;
     o += 4u * filter_words;
+    L.off_prof = o;  // section counters of the profiling build (kProfileBytes = 0 otherwise)
+    o += kProfileBytes;
     L.bytes = round16(o);
     return L;
 }
@@ -174,6 +176,11 @@ __device__ __forceinline__ void slide_to_start(uint64_t* keys, int from, int n, 
     }
 }
 
+#ifdef PGB_SECTION_PROFILE
+// the HNSW kernel's section totals (this translation unit's own device variable)
+static __device__ unsigned long long g_hnsw_section_cycles[NUM_SECTIONS];
+#endif
+
 // FMODE: where the lossy filter lives. 0: shared memory. 1: per-warp global table of ids
 // plus a shared-memory bitmap of the slots written on this layer (cleared per layer, so
 // unwritten slots need no load). 2: per-warp global table of (epoch, id) pairs, for
@@ -219,7 +226,15 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
         return __shfl_sync(kFull, v, 0);
     };
 
+#ifdef PGB_SECTION_PROFILE
+    unsigned long long* prof = reinterpret_cast<unsigned long long*>(wmem + L.off_prof);
+    if (lane < NUM_SECTIONS) prof[lane] = 0ull;
+    __syncwarp();
+#endif
+
     for (uint32_t q = take(); q < A.nq; q = take()) {
+        PGB_PROF_BEGIN(tp);
+        PGB_PROF_COUNT(SEC_QUERIES);
         load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
         __syncwarp();
         const int4* q4 = reinterpret_cast<const int4*>(qwords);
@@ -313,6 +328,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 unext = v;
             };
 
+            PGB_PROF_ADD(SEC_SETUP, tp);
             while (nC > 0) {
                 if (key_dist(ckey[c0]) > key_dist(wkey[nW - 1])) break;
                 if (++cnt > limit) break;
@@ -321,7 +337,9 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 nC--;
                 exps++;
                 uint32_t a[CH];
+                PGB_PROF_COUNT(SEC_ITERATIONS);
                 if (u == unext) {
+                    PGB_PROF_COUNT(SEC_PRED_HIT);
 #pragma unroll
                     for (int t = 0; t < CH; t++) a[t] = anext[t];
                 } else {
@@ -334,6 +352,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         a[t] = (j < G) ? __ldg(row + j) : kEmptyId;
                     }
                 }
+                PGB_PROF_ADD(SEC_VISIT, tp);
                 // ---- lossy visited filter in row order ---------------------------------
                 int np = 0;
                 if (SFILT) {
@@ -428,59 +447,78 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     }
                 }
                 comps += np;
+                PGB_PROF_COUNT_N(SEC_N_PENDING, np);
+                PGB_PROF_ADD(SEC_FILTER, tp);
                 row_distances<Signed>(A.rows, pend, pd, np, q4, qq, A.dim, A.norm_in_row != 0, lane);
+                PGB_PROF_ADD(SEC_DIST, tp);
 
-                // ---- eligibility: first copy in this expansion and not in is_inw ------
-                if (np <= 32) {
-                    // one chunk: earlier copies are the lanes below with the same id
-                    const uint32_t pv = lane < np ? pend[lane] : kEmptyId;
-                    const bool first = (__match_any_sync(kFull, pv) & lt) == 0;
-                    if (lane < np) {
-                        bool in_w = false;
-                        const uint32_t b = inw_bit(pv);
-                        if (first && ((ibits[b >> 5] >> (b & 31u)) & 1u))
-                            in_w = inw_contains(inw, occ, inw_mask, inw_shift, pv);
-                        fl[lane] = (first && !in_w) ? 1 : 0;
-                    }
-                } else {
-                    for (int j = lane; j < np; j += 32) {
-                        const uint32_t pv = pend[j];
-                        bool first = true;
-                        for (int i = 0; i < j; i++)
-                            if (pend[i] == pv) {
-                                first = false;
-                                break;
-                            }
-                        bool in_w = false;
-                        if (first) {
-                            const uint32_t b = inw_bit(pv);
-                            if ((ibits[b >> 5] >> (b & 31u)) & 1u)
-                                in_w = inw_contains(inw, occ, inw_mask, inw_shift, pv);
-                        }
-                        fl[j] = (first && !in_w) ? 1 : 0;
-                    }
-                }
-                __syncwarp();
-                // ---- acceptance: fewer than m elements of W + earlier eligible at <= d
+                // ---- eligibility (first copy in this expansion, not in is_inw) and
+                // acceptance (fewer than m elements of W + earlier eligible at <= d). With
+                // W full (nW >= ef, so m = nW) acceptance needs d < W's worst distance, and
+                // a neighbour at or beyond it never counts for one below it: only these
+                // "near" neighbours are checked at all. Copies of an id share a distance,
+                // so the first copy of a near id is near too.
                 const int m = max(ef, nW);
+                const int32_t worst = nW >= ef ? key_dist(wkey[nW - 1]) : INT_MAX;
                 int na = 0;
-                for (int base = 0; base < np; base += 32) {
-                    const int j = base + lane;
+                if (np <= 32) {
+                    // one chunk: earlier copies are the lanes below with the same id, and
+                    // the earlier eligible neighbours are a ballot mask
+                    const uint32_t pv = lane < np ? pend[lane] : kEmptyId;
+                    const int32_t dv = lane < np ? pd[lane] : INT_MAX;
+                    const bool first = (__match_any_sync(kFull, pv) & lt) == 0;
+                    bool elig = lane < np && dv < worst && first;
+                    if (elig) {
+                        const uint32_t b = inw_bit(pv);
+                        if ((ibits[b >> 5] >> (b & 31u)) & 1u)
+                            elig = !inw_contains(inw, occ, inw_mask, inw_shift, pv);
+                    }
+                    const uint32_t em = __ballot_sync(kFull, elig);
                     bool acc = false;
-                    int32_t d = 0;
-                    uint32_t pv = 0;
-                    if (j < np && fl[j]) {
-                        d = pd[j];
-                        pv = pend[j];
-                        int c = lower_bound_key(wkey, nW, pack_key(d + 1, 0));
-                        for (int i = 0; i < j && c < m; i++) c += (fl[i] && pd[i] <= d) ? 1 : 0;
+                    if (elig) {
+                        int c = lower_bound_key(wkey, nW, pack_key(dv + 1, 0));
+                        for (uint32_t mm = em & lt; mm != 0u && c < m; mm &= mm - 1u)
+                            c += pd[__ffs(mm) - 1] <= dv ? 1 : 0;
                         acc = c < m;
                     }
                     const uint32_t mk = __ballot_sync(kFull, acc);
-                    if (acc) akey[na + __popc(mk & lt)] = pack_key(d, pv);
-                    na += __popc(mk);
+                    if (acc) akey[__popc(mk & lt)] = pack_key(dv, pv);
+                    na = __popc(mk);
+                } else {
+                    for (int j = lane; j < np; j += 32) {
+                        const uint32_t pv = pend[j];
+                        bool elig = pd[j] < worst;
+                        for (int i = 0; i < j && elig; i++)
+                            if (pend[i] == pv) elig = false;
+                        if (elig) {
+                            const uint32_t b = inw_bit(pv);
+                            if ((ibits[b >> 5] >> (b & 31u)) & 1u)
+                                elig = !inw_contains(inw, occ, inw_mask, inw_shift, pv);
+                        }
+                        fl[j] = elig ? 1 : 0;
+                    }
+                    __syncwarp();
+                    for (int base = 0; base < np; base += 32) {
+                        const int j = base + lane;
+                        bool acc = false;
+                        int32_t d = 0;
+                        uint32_t pv = 0;
+                        if (j < np && fl[j]) {
+                            d = pd[j];
+                            pv = pend[j];
+                            int c = lower_bound_key(wkey, nW, pack_key(d + 1, 0));
+                            for (int i = 0; i < j && c < m; i++) c += (fl[i] && pd[i] <= d) ? 1 : 0;
+                            acc = c < m;
+                        }
+                        const uint32_t mk = __ballot_sync(kFull, acc);
+                        if (acc) akey[na + __popc(mk & lt)] = pack_key(d, pv);
+                        na += __popc(mk);
+                    }
                 }
                 __syncwarp();
+                PGB_PROF_COUNT_N(SEC_N_CAND, na);
+                if (na == 0) PGB_PROF_COUNT(SEC_NO_CAND);
+                PGB_PROF_ADD(SEC_SORT, tp);
                 if (na > 0) {
                     inserted += (uint32_t)na;
                     for (int j = lane; j < na; j += 32) {
@@ -569,6 +607,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     // the next expansion is cand's new closest entry: request its row now,
                     // while W is updated
                     if (nC > 0) request_row(key_id(ckey[c0]));
+                    PGB_PROF_ADD(SEC_UNION, tp);
                     // ---- W update: the m' smallest of W + accepted -----------------------
                     sort_keys<CH>(akey, na, lane);
                     const int nWn = min(m, nW + na);
@@ -592,6 +631,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         if (pos[j] < nWn) wkey[pos[j]] = akey[j];
                     __syncwarp();
                     nW = nWn;
+                    PGB_PROF_ADD(SEC_SHIFT, tp);
                 } else if (nC > 0) {
                     request_row(key_id(ckey[c0]));  // cand unchanged
                 }
@@ -599,6 +639,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     flags |= PGB_FLAG_OVERFLOW;
                     break;
                 }
+                PGB_PROF_ADD(SEC_CUT_NEXT, tp);
             }
             if (layer > 0) {
                 if (lane == 0) eps[0] = key_id(wkey[nW - 1]);
@@ -625,7 +666,12 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             A.stats[q] = s;
         }
         __syncwarp();
+        PGB_PROF_ADD(SEC_SETUP, tp);
     }
+#ifdef PGB_SECTION_PROFILE
+    __syncwarp();
+    if (lane < NUM_SECTIONS) atomicAdd(&g_hnsw_section_cycles[lane], prof[lane]);
+#endif
 }
 
 }  // namespace pgb
@@ -790,6 +836,24 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
                                      H.smem_bytes, stream);
     return hnsw_cuda(e, "HNSW launch");
+}
+
+cudaError_t hnsw_section_totals(unsigned long long* acc, bool reset) {
+#ifdef PGB_SECTION_PROFILE
+    unsigned long long v[NUM_SECTIONS];
+    cudaError_t e = cudaMemcpyFromSymbol(v, g_hnsw_section_cycles, sizeof(v));
+    if (e != cudaSuccess) return e;
+    for (int i = 0; i < NUM_SECTIONS; i++) acc[i] += v[i];
+    if (reset) {
+        unsigned long long zero[NUM_SECTIONS] = {0};
+        e = cudaMemcpyToSymbol(g_hnsw_section_cycles, zero, sizeof(zero));
+    }
+    return e;
+#else
+    (void)acc;
+    (void)reset;
+    return cudaSuccess;
+#endif
 }
 
 void hnsw_release(HnswState& H) {

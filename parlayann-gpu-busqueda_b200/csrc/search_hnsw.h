@@ -36,5 +36,8 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
                        const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
                        int32_t* dists, pgb_query_stats* stats, cudaStream_t stream);
 void hnsw_release(HnswState& H);
+// section totals of the HNSW kernel in the profiling build (added into acc; reset zeroes
+// them); a no-op otherwise
+cudaError_t hnsw_section_totals(unsigned long long* acc, bool reset);
 
 }  // namespace pgb
