@@ -17,6 +17,14 @@
 // ef smallest distinct distances of cand + accepted (first copy of each distance
 // wins); when cand starts above ef (several entry points on the top layer) its
 // per-neighbour trim rule is replayed sequentially instead.
+//
+// is_inw needs no table. Every id it receives on a layer also enters W, and once W is
+// full its worst key never grows, so an id that has left W has a key above W's current
+// worst. A neighbour that can be accepted has d < W's worst distance (or W is not full
+// and has lost nothing), hence for such a neighbour "in is_inw" is "in W", a lookup in
+// the sorted W already in shared memory; neighbours at or beyond the worst are never
+// looked up. Only the count of is_inw inserts is kept, for the overflow flag
+// (capInw / 2, busqueda_hnsw.cu:559).
 #include <algorithm>
 #include <climits>
 #include <string>
@@ -37,14 +45,10 @@ __host__ __device__ inline uint32_t hnsw_cap_inw(uint32_t Ls) {
 }
 
 struct HnswLayout {
-    uint32_t wcap, gs, filter_words, cap_inw, wbits_words;
-    uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_ibits,
-        off_occ, off_wbits, off_filter, off_prof, bytes;
+    uint32_t wcap, gs, filter_words, wbits_words;
+    uint32_t off_w, off_c, off_pend, off_pd, off_ak, off_nk, off_pos, off_fl, off_eps, off_wbits,
+        off_filter, off_prof, bytes;
 };
-
-// "maybe in is_inw" bitmap per warp: a clear bit proves absence, so most membership
-// checks never touch the global table
-constexpr uint32_t kInwBits = 4096;
 
 // The candidate list is a window ckey[c0, c0 + nC) that slides up as the closest entry is
 // popped; it is moved back to the start when an update would run past this capacity.
@@ -53,13 +57,11 @@ __host__ __device__ inline uint32_t hnsw_ccap(uint32_t wcap) { return 2u * wcap;
 // filter_words: shared-memory filter (FMODE 0); wbits_words: written-slot bitmap of a
 // global id filter (FMODE 1)
 __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t gs,
-                                                       uint32_t filter_words, uint32_t cap_inw,
-                                                       uint32_t wbits_words) {
+                                                       uint32_t filter_words, uint32_t wbits_words) {
     HnswLayout L;
     L.wcap = wcap;
     L.gs = gs;
     L.filter_words = filter_words;
-    L.cap_inw = cap_inw;
     L.wbits_words = wbits_words;
     uint32_t o = kRowBytes;
     L.off_w = o;
@@ -80,10 +82,6 @@ __host__ __device__ inline HnswLayout make_hnsw_layout(uint32_t wcap, uint32_t g
     o = round16(o + gs);
     L.off_eps = o;
     o += 4u * PGB_MAX_HNSW_ENTRIES;
-    L.off_ibits = o;
-    o += kInwBits / 8u;
-    L.off_occ = o;  // is_inw slot occupancy, one bit per slot (cap_inw is a power of two >= 4096)
-    o += cap_inw / 8u;
     L.off_wbits = o;
     o = round16(o + 4u * wbits_words);
     L.off_filter = o;
@@ -113,55 +111,28 @@ struct HnswArgs {
     uint32_t* ids;
     int32_t* dists;
     pgb_query_stats* stats;
-    uint32_t* inw;
     unsigned long long* gfilter;
     uint64_t epoch_base;
     uint32_t* queue;  // query work queue: each warp takes the next query when it is free
 };
 
-// is_inw is an exact set private to the search (only membership matters, not where ids
-// sit), so its slots come from cheap multiplicative hashes: Knuth's golden-ratio
-// constant for the home slot's top bits, a second odd constant for the maybe-bitmap.
-__device__ __forceinline__ uint32_t inw_bit(uint32_t id) {
-    return (id * 0x85EBCA6Bu) >> (32 - 12);  // kInwBits = 4096
-}
-__device__ __forceinline__ uint32_t inw_home(uint32_t id, uint32_t shift) {
-    return (id * 0x9E3779B1u) >> shift;
-}
-
 __device__ __forceinline__ unsigned long long tag(uint32_t epoch, uint32_t id) {
     return ((unsigned long long)epoch << 32) | id;
 }
 
-// is_inw membership: linear probing over the global id table, where a slot holds an id
-// of this layer iff its occupancy bit (shared memory, cleared per layer) is set; the
-// first clear bit of the run ends the search
-__device__ bool inw_contains(const uint32_t* tab, const uint32_t* occ, uint32_t mask,
-                             uint32_t shift, uint32_t id) {
-    uint32_t h = inw_home(id, shift);
-    for (uint32_t i = 0; i <= mask; i++) {
-        if (!((occ[h >> 5] >> (h & 31u)) & 1u)) return false;
-        if (__ldcg(tab + h) == id) return true;
-        h = (h + 1) & mask;
+// The number of W entries at distance <= d, and whether (d, id) is one of them: W is
+// sorted by (dist, id), so the entries at distance d follow the lower bound of (d, 0)
+__device__ __forceinline__ int w_count_le(const uint64_t* wkey, int nW, int32_t d, uint32_t id,
+                                          bool& in_w) {
+    int c = lower_bound_key(wkey, nW, pack_key(d, 0));
+    in_w = false;
+    while (c < nW) {
+        const uint64_t k = wkey[c];
+        if (key_dist(k) != d) break;
+        in_w |= key_id(k) == id;
+        c++;
     }
-    return false;
-}
-
-// insert of an id known to be absent, by any number of lanes at once (distinct ids): the
-// slot is claimed with a shared-memory atomic on its occupancy bit, then written without
-// waiting; lookups come after a __syncwarp, which orders the write before them. The
-// table never fills: a layer stops (overflow) once inserts pass half of it.
-__device__ void inw_insert(uint32_t* tab, uint32_t* occ, uint32_t mask, uint32_t shift,
-                           uint32_t id) {
-    uint32_t h = inw_home(id, shift);
-    for (uint32_t i = 0; i <= mask; i++) {
-        const uint32_t bit = 1u << (h & 31u);
-        if (!(occ[h >> 5] & bit) && !(atomicOr(&occ[h >> 5], bit) & bit)) {
-            tab[h] = id;
-            return;
-        }
-        h = (h + 1) & mask;
-    }
+    return c;
 }
 
 // moves keys[from, from + n) to keys[0, n) (from >= 0; chunk reads precede chunk writes)
@@ -205,16 +176,11 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     int32_t* pos = reinterpret_cast<int32_t*>(wmem + L.off_pos);
     uint8_t* fl = wmem + L.off_fl;
     uint32_t* eps = reinterpret_cast<uint32_t*>(wmem + L.off_eps);
-    uint32_t* ibits = reinterpret_cast<uint32_t*>(wmem + L.off_ibits);
-    uint32_t* occ = reinterpret_cast<uint32_t*>(wmem + L.off_occ);
     uint32_t* sfilter = reinterpret_cast<uint32_t*>(wmem + L.off_filter);
-    uint32_t* inw = A.inw + (size_t)gw * A.cap_inw;
     unsigned long long* gfil = FMODE == 2 ? A.gfilter + (size_t)gw * A.filter_slots : nullptr;
     uint32_t* gf32 = FMODE == 1 ? reinterpret_cast<uint32_t*>(A.gfilter) + (size_t)gw * A.filter_slots
                                 : nullptr;
     uint32_t* wbits = reinterpret_cast<uint32_t*>(wmem + L.off_wbits);
-    const uint32_t inw_mask = A.cap_inw - 1u;
-    const uint32_t inw_shift = 32u - (uint32_t)ceil_log2_u64(A.cap_inw);
     const int ccap = (int)hnsw_ccap(L.wcap);
     const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
     const uint32_t layers = A.top + 1u;
@@ -261,11 +227,6 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             } else if (FMODE == 1) {
                 for (uint32_t i = lane; i < (fmask + 32u) / 32u; i += 32) wbits[i] = 0u;
             }
-            // this layer's is_inw is empty: clear its maybe-bitmap (32 lanes x 16 bytes) and
-            // the slot occupancy bits (cap_inw / 128 16-byte words, a multiple of 32)
-            reinterpret_cast<uint4*>(ibits)[lane] = make_uint4(0, 0, 0, 0);
-            for (uint32_t i = lane; i < A.cap_inw / 128u; i += 32)
-                reinterpret_cast<uint4*>(occ)[i] = make_uint4(0, 0, 0, 0);
             __syncwarp();
             // ---- entry points: distances, then the sequential inserts on lane 0 ----
             for (int e = lane; e < neps; e += 32) pend[e] = eps[e];
@@ -286,11 +247,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     } else {
                         gfil[s] = tag(epoch, pe);
                     }
-                    // no membership test: a repeated entry point would take a second
-                    // slot, which changes no membership answer
-                    inw_insert(inw, occ, inw_mask, inw_shift, pe);
-                    const uint32_t b = inw_bit(pe);
-                    ibits[b >> 5] |= 1u << (b & 31u);
+                    // is_inw: W below holds every entry point (inserted without a
+                    // membership test, so a repeated entry point appears twice)
                     // cand: by distance, equal distance rejected
                     const uint64_t key = pack_key(d, pe);
                     int pos = lower_bound_key(ckey, nC, pack_key(d, 0));
@@ -468,15 +426,15 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                     const int32_t dv = lane < np ? pd[lane] : INT_MAX;
                     const bool first = (__match_any_sync(kFull, pv) & lt) == 0;
                     bool elig = lane < np && dv < worst && first;
+                    int c = 0;
                     if (elig) {
-                        const uint32_t b = inw_bit(pv);
-                        if ((ibits[b >> 5] >> (b & 31u)) & 1u)
-                            elig = !inw_contains(inw, occ, inw_mask, inw_shift, pv);
+                        bool in_w;
+                        c = w_count_le(wkey, nW, dv, pv, in_w);
+                        elig = !in_w;
                     }
                     const uint32_t em = __ballot_sync(kFull, elig);
                     bool acc = false;
                     if (elig) {
-                        int c = lower_bound_key(wkey, nW, pack_key(dv + 1, 0));
                         for (uint32_t mm = em & lt; mm != 0u && c < m; mm &= mm - 1u)
                             c += pd[__ffs(mm) - 1] <= dv ? 1 : 0;
                         acc = c < m;
@@ -491,9 +449,9 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                         for (int i = 0; i < j && elig; i++)
                             if (pend[i] == pv) elig = false;
                         if (elig) {
-                            const uint32_t b = inw_bit(pv);
-                            if ((ibits[b >> 5] >> (b & 31u)) & 1u)
-                                elig = !inw_contains(inw, occ, inw_mask, inw_shift, pv);
+                            bool in_w;
+                            w_count_le(wkey, nW, pd[j], pv, in_w);
+                            elig = !in_w;
                         }
                         fl[j] = elig ? 1 : 0;
                     }
@@ -520,13 +478,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 if (na == 0) PGB_PROF_COUNT(SEC_NO_CAND);
                 PGB_PROF_ADD(SEC_SORT, tp);
                 if (na > 0) {
-                    inserted += (uint32_t)na;
-                    for (int j = lane; j < na; j += 32) {
-                        const uint32_t id = key_id(akey[j]);
-                        inw_insert(inw, occ, inw_mask, inw_shift, id);
-                        const uint32_t b = inw_bit(id);
-                        atomicOr(&ibits[b >> 5], 1u << (b & 31u));
-                    }
+                    inserted += (uint32_t)na;  // is_inw inserts (the set itself is W)
                     // ---- cand update (accepted keys still in arrival order) ---------------
                     const int nC0 = nC;
                     uint64_t* cq = ckey + c0;
@@ -713,7 +665,7 @@ pgb_status hnsw_cuda(cudaError_t e, const char* what) {
 }  // namespace
 
 HnswLayout hnsw_layout_of(const HnswState& H) {
-    return make_hnsw_layout(H.wcap, 32u * H.ch, H.fmode == 0 ? (1u << H.bits0) : 0u, H.cap_inw,
+    return make_hnsw_layout(H.wcap, 32u * H.ch, H.fmode == 0 ? (1u << H.bits0) : 0u,
                             H.fmode == 1 ? H.filter_slots / 32u : 0u);
 }
 
@@ -760,10 +712,6 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     if (bps < 1) return fail(PGB_ERR_CUDA, "HNSW kernel does not fit on a multiprocessor");
     H.blocks = bps * prop.multiProcessorCount;
     H.total_warps = (uint64_t)H.blocks * wpb;
-    // is_inw ids; which slots hold this layer's ids is kept in shared memory, so the table
-    // needs no clearing
-    const size_t inw_bytes = 4ull * H.cap_inw * H.total_warps;
-    if ((s = hnsw_cuda(cudaMalloc(&H.inw, inw_bytes), "is_inw tables")) != PGB_OK) return s;
     if ((s = hnsw_cuda(cudaMalloc(&H.queue, sizeof(uint32_t)), "query queue")) != PGB_OK) return s;
     if (H.fmode == 1) {  // ids only; validity is the shared written-slot bitmap
         if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, 4ull * H.filter_slots * H.total_warps),
@@ -812,7 +760,6 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     A.ids = ids;
     A.dists = dists;
     A.stats = stats;
-    A.inw = H.inw;
     A.gfilter = H.gfilter;
     // every (query, layer) of every launch gets a fresh epoch for an (epoch, id) global
     // filter; wrap -> clear it
@@ -857,7 +804,6 @@ cudaError_t hnsw_section_totals(unsigned long long* acc, bool reset) {
 }
 
 void hnsw_release(HnswState& H) {
-    cudaFree(H.inw);
     cudaFree(H.gfilter);
     cudaFree(H.queue);
     H = HnswState{};

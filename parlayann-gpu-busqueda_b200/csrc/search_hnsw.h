@@ -16,7 +16,7 @@ struct HnswState {
     int ch = 1;
     int fmode = 0;              // lossy filter: 0 shared, 1 global ids + shared bitmap, 2 global (epoch, id)
     uint32_t bits0 = 2;         // layer-0 filter bits
-    uint32_t cap_inw = 0;       // is_inw slots (power of two)
+    uint32_t cap_inw = 0;       // the reference's is_inw capacity: overflow past half of it
     uint32_t filter_slots = 0;  // global filter slots per warp (0: shared)
     uint32_t wcap = 0;          // workset / candidate capacity
     uint32_t warp_bytes = 0;
@@ -24,7 +24,6 @@ struct HnswState {
     uint64_t total_warps = 0;
     size_t smem_bytes = 0;
     void* kernel = nullptr;
-    uint32_t* inw = nullptr;               // is_inw ids per warp (slot validity in shared memory)
     unsigned long long* gfilter = nullptr; // global lossy filter per warp: 4-byte ids
                                            // (fmode 1) or (epoch, id) pairs (fmode 2)
     uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
