@@ -9,6 +9,8 @@
 //   ids, dists = idx.batch_search(queries, knn=10, beam_size=40, cut=1.35, limit=-1)
 //   hidx = _pgbpy.HNSWIndex("base.i8bin", "model.hnsw", "int8")
 //   deg, edges = _pgbpy.build_vamana(x, R=64, L=128, alpha=1.2)   # GPU construction
+//   deg, edges = _pgbpy.build_hcnng(x, trees=30, leaf=1000, mst_deg=3)
+//   _pgbpy.build_hnsw(x, "model.hnsw", M=32, ef_construction=128)
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 
@@ -121,6 +123,38 @@ py::tuple build_vamana(py::array x, uint32_t R, uint32_t L, float alpha, int pas
     return py::make_tuple(deg, adj);
 }
 
+py::tuple build_hcnng(py::array x, uint32_t trees, uint32_t leaf, uint32_t mst_deg, uint64_t seed,
+                      int device) {
+    auto a = py::array::ensure(x, py::array::c_style);
+    if (!a || a.ndim() != 2 || a.itemsize() != 1) throw std::invalid_argument("x: a 2-d 8-bit array");
+    const pgb_elem e = a.dtype().kind() == 'i' ? PGB_INT8 : PGB_UINT8;
+    const uint32_t n = (uint32_t)a.shape(0), d = (uint32_t)a.shape(1);
+    py::array_t<uint32_t> deg(n);
+    py::array_t<uint32_t> adj({(py::ssize_t)n, (py::ssize_t)trees * mst_deg});
+    pgb_status rc;
+    {
+        py::gil_scoped_release nogil;
+        rc = pgb_build_hcnng_gpu(device, a.data(), n, d, e, trees, leaf, mst_deg, seed,
+                                 deg.mutable_data(), adj.mutable_data());
+    }
+    check(rc);
+    return py::make_tuple(deg, adj);
+}
+
+void build_hnsw(py::array x, const std::string& path, uint32_t M, uint32_t ef_construction, float ml,
+                float alpha, uint64_t seed, int device) {
+    auto a = py::array::ensure(x, py::array::c_style);
+    if (!a || a.ndim() != 2 || a.itemsize() != 1) throw std::invalid_argument("x: a 2-d 8-bit array");
+    const pgb_elem e = a.dtype().kind() == 'i' ? PGB_INT8 : PGB_UINT8;
+    pgb_status rc;
+    {
+        py::gil_scoped_release nogil;
+        rc = pgb_build_hnsw_gpu(device, a.data(), (uint32_t)a.shape(0), (uint32_t)a.shape(1), e, M,
+                                ef_construction, ml, alpha, seed, path.c_str());
+    }
+    check(rc);
+}
+
 double compute_recall(py::array_t<uint32_t, py::array::c_style> gt_ids,
                       py::array_t<float, py::array::c_style> gt_dists,
                       py::array_t<uint32_t, py::array::c_style> ids, uint32_t k) {
@@ -152,6 +186,13 @@ PYBIND11_MODULE(_pgbpy, m) {
     m.def("build_vamana", &build_vamana, py::arg("x"), py::arg("R") = 64, py::arg("L") = 128,
           py::arg("alpha") = 1.2f, py::arg("passes") = 1, py::arg("seed") = 0, py::arg("device") = 0,
           "GPU Vamana construction: (degrees [n], adjacency [n, R] padded with 0xFFFFFFFF)");
+    m.def("build_hcnng", &build_hcnng, py::arg("x"), py::arg("trees") = 30, py::arg("leaf") = 1000,
+          py::arg("mst_deg") = 3, py::arg("seed") = 0, py::arg("device") = 0,
+          "GPU HCNNG construction: (degrees [n], adjacency [n, trees * mst_deg])");
+    m.def("build_hnsw", &build_hnsw, py::arg("x"), py::arg("path"), py::arg("M") = 32,
+          py::arg("ef_construction") = 128, py::arg("ml") = 0.36f, py::arg("alpha") = 0.83f,
+          py::arg("seed") = 0, py::arg("device") = 0,
+          "GPU HNSW construction, written to an HNSW v3 model file at path");
     m.def("compute_recall", &compute_recall, py::arg("gt_ids"), py::arg("gt_dists"), py::arg("ids"),
           py::arg("k"), "recall@k with distance ties (the reference's calcularRecall)");
 }

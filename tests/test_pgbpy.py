@@ -1,5 +1,6 @@
 """_pgbpy, the pybind11 module for big-ann-benchmarks-style harnesses: an index loaded from
-the reference's files, batch_search on numpy arrays, GPU Vamana construction, recall."""
+the reference's files, batch_search on numpy arrays, GPU Vamana / HCNNG / HNSW construction,
+recall."""
 import os
 import sys
 
@@ -19,7 +20,8 @@ def pgbpy(pgb):
 
 
 def test_module_surface(pgbpy):
-    for name in ("FlatIndex", "HNSWIndex", "Index", "build_vamana", "compute_recall"):
+    for name in ("FlatIndex", "HNSWIndex", "Index", "build_vamana", "build_hcnng", "build_hnsw",
+                 "compute_recall"):
         assert hasattr(pgbpy, name), name
 
 
@@ -64,3 +66,16 @@ def test_build_vamana_equals_cpu_builder(pgb, pgbpy, golden, gpu):
     g = pgb.Graph.from_padded(deg, adj)
     assert_same("degrees", g.degrees, c.degrees)
     assert_same("edges", g.edges, c.edges)
+
+
+@pytest.mark.gpu
+def test_build_hcnng_and_hnsw_equal_cpu_builders(pgb, pgbpy, golden, gpu, tmp_path):
+    deg, adj = pgbpy.build_hcnng(golden.base, trees=4, leaf=300, mst_deg=3, seed=1)
+    c = pgb.build_hcnng(golden.base, trees=4, leaf=300, mst_deg=3, seed=1)
+    g = pgb.Graph.from_padded(deg, adj)
+    assert_same("hcnng degrees", g.degrees, c.degrees)
+    assert_same("hcnng edges", g.edges, c.edges)
+    pg, pc = str(tmp_path / "g.hnsw"), str(tmp_path / "c.hnsw")
+    pgbpy.build_hnsw(golden.base, pg, M=8, ef_construction=32, ml=0.5, alpha=1.0, seed=0)
+    pgb.build_hnsw(golden.base, pc, M=8, ef_construction=32, ml=0.5, alpha=1.0, seed=0)
+    assert open(pg, "rb").read() == open(pc, "rb").read()
