@@ -358,12 +358,14 @@ def main():
     ap.add_argument("--profile-nq", type=int, default=8192)
     ap.add_argument("--profile-ls", type=int, default=40)
     ap.add_argument("--workload", default="vamana",
-                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving", "c4", "build"],
+                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving", "serving_hnsw",
+                             "c4", "build"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
-                         "mixed: 100k queries of uneven Ls and k in one launch; serving: "
-                         "Poisson bursts through the request loop; c4: 10M uint8 d=128 "
-                         "Vamana, 100k queries, Ls 20/50/100/200; build: GPU vs CPU Vamana "
+                         "mixed: 100k queries of uneven Ls and k in one launch; serving / "
+                         "serving_hnsw: Poisson bursts through the request loop on the Vamana "
+                         "graph / the HNSW model; c4: 10M uint8 d=128 Vamana, 100k queries, "
+                         "Ls 20/50/100/200; build: GPU vs CPU Vamana, HNSW and HCNNG "
                          "construction on the 1M base")
     args = ap.parse_args()
     rank, world, local = dist_env()
@@ -373,8 +375,9 @@ def main():
         else:
             run_profile(args, local)
         return
-    if args.workload in ("hnsw", "mixed", "serving", "c4", "build") and args.impl == "ours":
-        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving, "c4": run_c4,
+    if args.workload in ("hnsw", "mixed", "serving", "serving_hnsw", "c4", "build") and args.impl == "ours":
+        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving,
+         "serving_hnsw": lambda a, lo: run_serving(a, lo, "hnsw"), "c4": run_c4,
          "build": run_build}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
@@ -877,15 +880,21 @@ def run_mixed(args, local):
         "gpu_launches": steps + len(plain)}), flush=True)
 
 
-def run_serving(args, local):
+def run_serving(args, local, kind="vamana"):
     """Poisson arrivals of single queries and bursts (1-256) at offered rates from 10k to
-    2M QPS through the request loop; per-request Ls in {20,50,100,300}, k in {10,100}."""
+    2M QPS through the request loop; per-request Ls in {20,50,100,300}, k in {10,100}; on
+    the Vamana graph or (kind "hnsw") the HNSW model of the same base."""
     import torch
     torch.cuda.set_device(local)
     pgb = ge.load_package()
-    base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana")
+    if kind == "hnsw":
+        base, h = load_hnsw(pgb)
+        queries = rank_queries(0)
+        index = pgb.Index.hnsw(base, h, device=local)
+    else:
+        base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana")
+        index = pgb.Index.flat(base, graph, device=local)
     gt_ids, gt_d = ground_truth(base, queries, 0, local)
-    index = pgb.Index.flat(base, graph, device=local)
     rng = np.random.default_rng(1)
     rates = [int(r) for r in os.environ.get("PGB_SERVE_RATES",
                                             "10000,100000,500000,1000000,2000000").split(",")]
@@ -953,8 +962,9 @@ def run_serving(args, local):
         "value": best["sustained_qps"], "unit": "queries/s", "n_gpus": 1, "steps": len(rows),
         "warmup": 0, "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-        "config": {"workload": "1M int8 d=100 Vamana R64, per-request Ls in {20,50,100,300}, k in "
-                               "{10,100}, bursts of 1-256", "rates": rows},
+        "config": {"workload": "1M int8 d=100 %s, per-request Ls in {20,50,100,300}, k in "
+                               "{10,100}, bursts of 1-256" % ("HNSW M32 efc128" if kind == "hnsw"
+                                                               else "Vamana R64"), "rates": rows},
         "gpu_launches": int(sum(r["launches"] for r in rows))}), flush=True)
 
 

@@ -226,13 +226,15 @@ pgb_status pgb_batch_replay(pgb_batch* b, void* stream);
 pgb_status pgb_batch_destroy(pgb_batch* b);
 
 /* ---- serving (no counterpart in the reference) ----------------------------------------
- * A request loop over one flat-graph index. submit() copies the query and admits the
- * request into a bounded pool (PGB_ERR_BUSY when full; the pool is sized by the device
+ * A request loop over one flat-graph or HNSW index. submit() copies the query and admits
+ * the request into a bounded pool (PGB_ERR_BUSY when full; the pool is sized by the device
  * memory budget). A dispatcher thread continuously packs whatever has arrived into
  * batches (longest beam first) and launches them on up to max_inflight streams, so
  * requests that arrive while others are on the GPU start as soon as a stream and slots
- * free up, overlapping with them. Each request gets exactly the neighbours that
- * pgb_searcher_search returns for it alone with the same params (exclusion quirk off). */
+ * free up, overlapping with them (on an HNSW index too, each request at its own beam
+ * and k). Each request gets exactly the neighbours that pgb_searcher_search returns
+ * for it alone with the same params (exclusion quirk off; cut and degree_limit apply to
+ * flat graphs). */
 typedef struct pgb_server_options {
     uint32_t max_beam;       /* largest beam a request may ask for                       */
     uint32_t max_k;          /* largest k a request may ask for                          */

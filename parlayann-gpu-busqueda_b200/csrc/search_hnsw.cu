@@ -114,6 +114,12 @@ struct HnswArgs {
     unsigned long long* gfilter;
     uint64_t epoch_base;
     uint32_t* queue;  // query work queue: each warp takes the next query when it is free
+    uint32_t out_stride;  // query q's k outputs start at q * out_stride
+    // batched launch (else null): query q's beam and k, and the order the queue hands the
+    // queries out in (longest beam first)
+    const uint32_t* ls_arr;
+    const uint32_t* k_arr;
+    const uint32_t* order;
 };
 
 __device__ __forceinline__ unsigned long long tag(uint32_t epoch, uint32_t id) {
@@ -198,7 +204,16 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     __syncwarp();
 #endif
 
-    for (uint32_t q = take(); q < A.nq; q = take()) {
+    for (uint32_t t = take(); t < A.nq; t = take()) {
+        const uint32_t q = A.order ? A.order[t] : t;
+        // this query's beam, k, layer-0 filter bits and is_inw overflow threshold
+        uint32_t qLs = A.Ls, qk = A.k, qbits0 = A.bits0, qcap_half = A.cap_inw / 2;
+        if (A.ls_arr) {
+            qLs = A.ls_arr[q];
+            qk = A.k_arr[q];
+            qbits0 = hnsw_bits0(qLs);
+            qcap_half = hnsw_cap_inw(qLs) / 2;
+        }
         PGB_PROF_BEGIN(tp);
         PGB_PROF_COUNT(SEC_QUERIES);
         load_query_row(A.queries + (size_t)q * A.qstride, A.dim, lane, qwords);
@@ -213,8 +228,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
         int nW = 0;
 
         for (int layer = (int)A.top; layer >= 0; layer--) {
-            const int ef = (layer > 0) ? 1 : (int)A.Ls;
-            const uint32_t bits = (layer > 0) ? 2u : A.bits0;
+            const int ef = (layer > 0) ? 1 : (int)qLs;
+            const uint32_t bits = (layer > 0) ? 2u : qbits0;
             const uint32_t fmask = (1u << bits) - 1u;
             const uint64_t limit = (layer > 0) ? ~0ull : A.limit0;
             const uint32_t* mat = (layer > 0) ? A.adju : A.adj0;
@@ -587,7 +602,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 } else if (nC > 0) {
                     request_row(key_id(ckey[c0]));  // cand unchanged
                 }
-                if (inserted > A.cap_inw / 2) {
+                if (inserted > qcap_half) {
                     flags |= PGB_FLAG_OVERFLOW;
                     break;
                 }
@@ -600,10 +615,10 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             }
         }
         // ---- output: first k of W, node -> point ------------------------------------
-        if (nW < (int)A.k) flags |= PGB_FLAG_SHORT;
-        uint32_t* oid = A.ids + (size_t)q * A.k;
-        int32_t* od = A.dists + (size_t)q * A.k;
-        for (uint32_t j = lane; j < A.k; j += 32) {
+        if (nW < (int)qk) flags |= PGB_FLAG_SHORT;
+        uint32_t* oid = A.ids + (size_t)q * A.out_stride;
+        int32_t* od = A.dists + (size_t)q * A.out_stride;
+        for (uint32_t j = lane; j < qk; j += 32) {
             const bool have = (int)j < nW;
             const uint64_t e = have ? wkey[j] : 0;
             oid[j] = have ? A.node_point[key_id(e)] : kEmptyId;
@@ -723,6 +738,7 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
         if ((s = hnsw_cuda(cudaMemset(H.gfilter, 0, fb), "filter clear")) != PGB_OK) return s;
     }
     H.epoch_base = 0;
+    H.max_ls = Ls;
     H.ready = true;
     return PGB_OK;
 }
@@ -730,8 +746,27 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
 pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params& p,
                        const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
                        int32_t* dists, pgb_query_stats* stats, cudaStream_t stream) {
+    return hnsw_launch_at(ix, H, p.beam_size, p.k, p.limit, queries, nq, qstride, ids, dists, stats,
+                          p.k, stream);
+}
+
+size_t hnsw_scratch_bytes(const HnswState& H) {
+    const size_t per_slot = H.fmode == 1 ? 4 : H.fmode == 2 ? 8 : 0;
+    return per_slot * H.filter_slots * H.total_warps + sizeof(uint32_t);
+}
+
+pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32_t k, int64_t limit,
+                          const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
+                          int32_t* dists, pgb_query_stats* stats, uint32_t out_stride,
+                          cudaStream_t stream, const uint32_t* ls_arr, const uint32_t* k_arr,
+                          const uint32_t* order) {
     if (!H.ready) return fail(PGB_ERR_BAD_ARG, "HNSW searcher not prepared");
+    if (Ls == 0 || Ls > H.max_ls || k == 0 || out_stride < k || (ls_arr == nullptr) != (k_arr == nullptr))
+        return fail(PGB_ERR_BAD_ARG, "HNSW launch: beam above the prepared one, or bad k / stride");
     HnswArgs A{};
+    A.ls_arr = ls_arr;
+    A.k_arr = k_arr;
+    A.order = order;
     A.rows = ix->node_rows;
     A.adj0 = ix->adj0;
     A.g0s = ix->g0s;
@@ -749,12 +784,15 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
     A.queries = (const uint8_t*)queries;
     A.nq = nq;
     A.qstride = qstride;
-    A.Ls = p.beam_size;
-    A.k = p.k;
+    A.Ls = Ls;
+    A.k = k;
+    A.out_stride = out_stride;
     // limit_eval on layer 0: the visit limit when set below n, else n (busqueda_hnsw.cu:610)
-    A.limit0 = (p.limit > 0 && (uint64_t)p.limit < ix->n_nodes) ? (uint64_t)p.limit : ix->n_nodes;
-    A.bits0 = H.bits0;
-    A.cap_inw = H.cap_inw;
+    A.limit0 = (limit > 0 && (uint64_t)limit < ix->n_nodes) ? (uint64_t)limit : ix->n_nodes;
+    // the filter and is_inw capacity of this beam; the tables (sized for H.max_ls, with
+    // its filter placement) hold them
+    A.bits0 = hnsw_bits0(Ls);
+    A.cap_inw = hnsw_cap_inw(Ls);
     A.filter_slots = H.filter_slots;
     A.L = hnsw_layout_of(H);
     A.ids = ids;

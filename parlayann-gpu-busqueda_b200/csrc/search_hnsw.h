@@ -27,6 +27,7 @@ struct HnswState {
     unsigned long long* gfilter = nullptr; // global lossy filter per warp: 4-byte ids
                                            // (fmode 1) or (epoch, id) pairs (fmode 2)
     uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
+    uint32_t max_ls = 0;                   // the beam the state was prepared for
     uint32_t* queue = nullptr;             // next query of the running launch (zeroed per launch)
 };
 
@@ -34,6 +35,17 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
 pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params& p,
                        const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
                        int32_t* dists, pgb_query_stats* stats, cudaStream_t stream);
+// One launch at beam Ls <= H.max_ls and k, the outputs of query q at q * out_stride (the
+// filter size and is_inw capacity follow Ls; the tables were sized for H.max_ls). With
+// ls_arr / k_arr (device, every beam <= H.max_ls, every k <= out_stride) query q runs at
+// its own beam and k, and the work queue hands the queries out in `order` (may be null).
+pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32_t k, int64_t limit,
+                          const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
+                          int32_t* dists, pgb_query_stats* stats, uint32_t out_stride,
+                          cudaStream_t stream, const uint32_t* ls_arr = nullptr,
+                          const uint32_t* k_arr = nullptr, const uint32_t* order = nullptr);
+// device bytes of the state's scratch tables
+size_t hnsw_scratch_bytes(const HnswState& H);
 void hnsw_release(HnswState& H);
 // section totals of the HNSW kernel in the profiling build (added into acc; reset zeroes
 // them); a no-op otherwise

@@ -1,4 +1,6 @@
-// server.cu -- pgb_server_*: a continuous-batching request loop over a flat-graph index.
+// server.cu -- pgb_server_*: a continuous-batching request loop over a flat-graph or an
+// HNSW index. (HNSW: each context holds an HNSW searcher state prepared for max_beam, and a
+// batch runs as one HNSW launch with each query at its own (Ls, k).)
 //
 // Host side: submit() admits a request into a bounded slot pool (busy when full) and
 // wakes the dispatcher thread. The dispatcher completes finished launches (event query),
@@ -31,6 +33,7 @@
 
 #include "errors.h"
 #include "index.h"
+#include "search_hnsw.h"
 #include "search_plan.h"
 #include "searcher.h"
 
@@ -68,6 +71,7 @@ struct Context {
     uint32_t* d_queue = nullptr;
     uint32_t* gfilter = nullptr;
     uint32_t* gvisited = nullptr;
+    HnswState hnsw;  // HNSW index: this context's searcher state, prepared for max_beam
 };
 
 constexpr size_t kLatencyRing = 65536;
@@ -79,6 +83,8 @@ struct pgb_server {
     pgb_index* index = nullptr;
     pgb_server_options opt{};
     pgb::FlatPlan plan{};
+    bool hnsw = false;            // HNSW index: per-(Ls, k) launches of the HNSW kernel
+    size_t hnsw_scratch = 0;      // device bytes of one context's HNSW state
     uint32_t deg_lim = 0;
     size_t in_q_bytes = 0, in_bytes = 0;  // staging layout
     std::vector<pgb::Context> ctx;
@@ -117,7 +123,18 @@ void free_context(Context& c) {
     cudaFree(c.d_queue);
     cudaFree(c.gfilter);
     cudaFree(c.gvisited);
+    hnsw_release(c.hnsw);
     c = Context{};
+}
+
+// the searcher parameters an HNSW context is prepared with (the largest request)
+pgb_query_params hnsw_params(const pgb_server* S) {
+    pgb_query_params p{};
+    p.k = S->opt.max_k;
+    p.beam_size = S->opt.max_beam;
+    p.cut = S->opt.cut;
+    p.limit = S->opt.limit;
+    return p;
 }
 
 pgb_status alloc_context(pgb_server* S, Context& c) {
@@ -135,6 +152,10 @@ pgb_status alloc_context(pgb_server* S, Context& c) {
         (s = cuda_status(cudaMalloc(&c.d_stats, sizeof(pgb_query_stats) * mb), "device outputs")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&c.d_queue, 4), "queue counter")) != PGB_OK)
         return s;
+    if (S->hnsw) {
+        const pgb_query_params p = hnsw_params(S);
+        return hnsw_prepare(S->index, p, c.hnsw);
+    }
     const uint64_t tw = S->plan.total_warps;
     if (S->plan.gfilter_words &&
         (s = cuda_status(cudaMalloc(&c.gfilter, 4ull * S->plan.gfilter_words * tw), "filter scratch")) != PGB_OK)
@@ -147,8 +168,9 @@ pgb_status alloc_context(pgb_server* S, Context& c) {
 
 size_t context_device_bytes(const pgb_server* S) {
     const size_t mb = S->opt.max_batch, mk = S->opt.max_k, tw = S->plan.total_warps;
-    return S->in_bytes + 8 * mb * mk + sizeof(pgb_query_stats) * mb + 4 +
-           4ull * (S->plan.gfilter_words + S->plan.gvisited_words) * tw;
+    const size_t staging = S->in_bytes + 8 * mb * mk + sizeof(pgb_query_stats) * mb + 4;
+    if (S->hnsw) return staging + S->hnsw_scratch;
+    return staging + 4ull * (S->plan.gfilter_words + S->plan.gvisited_words) * tw;
 }
 
 // called with the lock held
@@ -163,6 +185,24 @@ void set_failed(pgb_server* S, pgb_status s, const std::string& m) {
 void fail_unlocked(pgb_server* S, pgb_status s, const std::string& m) {
     std::lock_guard<std::mutex> lk(S->mu);
     set_failed(S, s, m);
+}
+
+// downloads a launched batch's outputs and records its completion event
+bool download(pgb_server* S, Context& c, uint32_t b) {
+    const size_t mk = S->opt.max_k;
+    cudaError_t e = cudaMemcpyAsync(c.h_ids, c.d_ids, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c.h_dists, c.d_dists, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(c.h_stats, c.d_stats, sizeof(pgb_query_stats) * b,
+                            cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail_unlocked(S, PGB_ERR_CUDA, std::string("server launch: ") + cudaGetErrorString(e));
+        return false;
+    }
+    return true;
 }
 
 // packs c.slots (taken from the pending queue under the lock) and launches them; runs
@@ -188,6 +228,17 @@ bool launch(pgb_server* S, Context& c) {
         cudaGetLastError();
         fail_unlocked(S, PGB_ERR_CUDA, std::string("server upload: ") + cudaGetErrorString(e));
         return false;
+    }
+    const uint32_t* d_ls = reinterpret_cast<const uint32_t*>(c.d_in + S->in_q_bytes);
+    if (S->hnsw) {
+        // one launch of the HNSW kernel: each query at its own (Ls, k), longest beam first
+        if (hnsw_launch_at(ix, c.hnsw, S->opt.max_beam, S->opt.max_k, S->opt.limit, c.d_in, b, ix->dim,
+                           c.d_ids, c.d_dists, c.d_stats, S->opt.max_k, c.stream, d_ls, d_ls + mb,
+                           d_ls + 2 * mb) != PGB_OK) {
+            fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
+            return false;
+        }
+        return download(S, c, b);
     }
     FlatArgs A{};
     A.rows = ix->rows;
@@ -219,20 +270,7 @@ bool launch(pgb_server* S, Context& c) {
         fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
         return false;
     }
-    const size_t mk = S->opt.max_k;
-    e = cudaMemcpyAsync(c.h_ids, c.d_ids, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(c.h_dists, c.d_dists, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(c.h_stats, c.d_stats, sizeof(pgb_query_stats) * b,
-                            cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        fail_unlocked(S, PGB_ERR_CUDA, std::string("server launch: ") + cudaGetErrorString(e));
-        return false;
-    }
-    return true;
+    return download(S, c, b);
 }
 
 // publishes a finished launch: results into the slots (no lock), then counters
@@ -380,7 +418,6 @@ pgb_status pgb_server_create(pgb_index* ix, const pgb_server_options* opt, pgb_s
     if (!out) return fail(PGB_ERR_BAD_ARG, "null output handle");
     *out = nullptr;
     if (!ix || !opt) return fail(PGB_ERR_BAD_ARG, "null index or options");
-    if (ix->is_hnsw) return fail(PGB_ERR_BAD_ARG, "the server serves flat graphs");
     if (opt->max_beam == 0 || opt->max_beam > PGB_MAX_BEAM || opt->max_k == 0 ||
         opt->max_k > PGB_MAX_K || !(opt->cut > 0))
         return fail(PGB_ERR_BAD_ARG, "bad max_beam / max_k / cut");
@@ -391,16 +428,31 @@ pgb_status pgb_server_create(pgb_index* ix, const pgb_server_options* opt, pgb_s
     S->opt = *opt;
     if (S->opt.max_batch == 0) S->opt.max_batch = 1024;
     if (S->opt.max_inflight == 0) S->opt.max_inflight = 4;
-    S->deg_lim = opt->degree_limit ? std::min(opt->degree_limit, ix->G) : ix->G;
-    FlatPlanRequest rq;
-    rq.max_ls = S->opt.max_beam;
-    rq.deg_lim = S->deg_lim;
-    rq.is_signed = ix->elem == PGB_INT8;
-    rq.batched = true;
-    pgb_status s = plan_flat(rq, S->plan);
-    if (s != PGB_OK) {
-        delete S;
-        return s;
+    pgb_status s;
+    S->hnsw = ix->is_hnsw;
+    if (S->hnsw) {
+        // one context's HNSW tables, measured on a probe state
+        HnswState probe;
+        const pgb_query_params p = hnsw_params(S);
+        if ((s = hnsw_prepare(ix, p, probe)) != PGB_OK) {
+            hnsw_release(probe);
+            delete S;
+            return s;
+        }
+        S->hnsw_scratch = hnsw_scratch_bytes(probe);
+        hnsw_release(probe);
+    } else {
+        S->deg_lim = opt->degree_limit ? std::min(opt->degree_limit, ix->G) : ix->G;
+        FlatPlanRequest rq;
+        rq.max_ls = S->opt.max_beam;
+        rq.deg_lim = S->deg_lim;
+        rq.is_signed = ix->elem == PGB_INT8;
+        rq.batched = true;
+        s = plan_flat(rq, S->plan);
+        if (s != PGB_OK) {
+            delete S;
+            return s;
+        }
     }
     const size_t mb = S->opt.max_batch;
     S->in_q_bytes = align16(mb * ix->dim);

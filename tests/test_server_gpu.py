@@ -99,3 +99,32 @@ def test_server_rejects_bad_requests(pgb, golden, gpu):
     with pytest.raises(pgb.PgbError):
         server.submit(queries[0], 40, 11)
     server.close()
+
+
+def test_hnsw_requests_match_oracle_in_the_mix(pgb, oracle, golden, gpu):
+    """HNSW serving: a batch runs as one launch with each query at its own (Ls, k), on
+    tables prepared for max_beam (300: the global (epoch, id) filter) -- every request
+    still gets the oracle's answer for its own Ls and k."""
+    base, queries = golden.vectors_for("hnsw")
+    h = golden.hnsw["hnsw"]
+    index = pgb.Index.hnsw(base, h)
+    rng = np.random.default_rng(11)
+    nq = len(queries)
+    ls = rng.choice([10, 50, 100, 300], size=nq)
+    ks = rng.choice([10, 20], size=nq)
+    server = pgb.Server(index, max_beam=300, max_k=20, max_batch=48, max_inflight=2)
+    tickets = {}
+    for i in range(nq):
+        t = None
+        while t is None:
+            t = server.submit(queries[i], int(ls[i]), int(ks[i]))
+        tickets[i] = t
+    got = drain(server, tickets, ks)
+    st = server.stats()
+    for i in range(nq):
+        oi, od, *_ = oracle.hnsw_search(base, h, queries[i][None], int(ks[i]), int(ls[i]))
+        assert_same(f"ids q{i}", got[i][0], oi[0])
+        assert_same(f"dists q{i}", got[i][1], od[0])
+    assert st["completed"] == nq and st["launches"] < nq
+    server.close()
+    index.close()
