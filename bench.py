@@ -58,12 +58,13 @@ def dist_env():
 
 
 # the four graph families of the 1M workload, as the reference's runs name them; Vamana
-# graphs come from the GPU builder, whose graph is the CPU builder's (tests/test_build_gpu.py)
+# and HCNNG graphs come from the GPU builders, whose graphs are the CPU builders'
+# (tests/test_build_gpu.py)
 GRAPHS = {
     "vamana": ("c2_vamana_R64_L128_a1.2.graph", "Vamana R64 L128 alpha1.2",
                lambda pgb, x: pgb.build_vamana_gpu(x, R=R, L=L_BUILD, alpha=ALPHA, seed=0)),
     "hcnng": ("c2_hcnng_T30_L1000_m3.graph", "HCNNG 30 trees leaf1000 MST3",
-              lambda pgb, x: pgb.build_hcnng(x, trees=30, leaf=1000, mst_deg=3, seed=0)),
+              lambda pgb, x: pgb.build_hcnng_gpu(x, trees=30, leaf=1000, mst_deg=3, seed=0)),
     "nnd": ("c2_nnd_K40.graph", "PyNNDescent K40 alpha1.2",
             lambda pgb, x: pgb.build_nndescent(x, K=40, init_trees=10, leaf=1000, alpha=1.2,
                                                seed=0)),
@@ -358,11 +359,12 @@ def main():
     ap.add_argument("--profile-nq", type=int, default=8192)
     ap.add_argument("--profile-ls", type=int, default=40)
     ap.add_argument("--workload", default="vamana",
-                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "serving", "serving_hnsw",
-                             "c4", "build"],
+                    choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "mixed_hnsw", "serving",
+                             "serving_hnsw", "c4", "build"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
-                         "mixed: 100k queries of uneven Ls and k in one launch; serving / "
+                         "mixed / mixed_hnsw: 100k queries of uneven Ls and k in one launch "
+                         "on the Vamana graph / the HNSW model; serving / "
                          "serving_hnsw: Poisson bursts through the request loop on the Vamana "
                          "graph / the HNSW model; c4: 10M uint8 d=128 Vamana, 100k queries, "
                          "Ls 20/50/100/200; build: GPU vs CPU Vamana, HNSW and HCNNG "
@@ -375,8 +377,10 @@ def main():
         else:
             run_profile(args, local)
         return
-    if args.workload in ("hnsw", "mixed", "serving", "serving_hnsw", "c4", "build") and args.impl == "ours":
-        {"hnsw": run_hnsw, "mixed": run_mixed, "serving": run_serving,
+    if args.workload in ("hnsw", "mixed", "mixed_hnsw", "serving", "serving_hnsw", "c4",
+                         "build") and args.impl == "ours":
+        {"hnsw": run_hnsw, "mixed": run_mixed, "mixed_hnsw": lambda a, lo: run_mixed(a, lo, "hnsw"),
+         "serving": run_serving,
          "serving_hnsw": lambda a, lo: run_serving(a, lo, "hnsw"), "c4": run_c4,
          "build": run_build}[args.workload](args, local)
         return
@@ -819,20 +823,27 @@ def run_c4(args, local):
         "gpu_launches": 2 * args.steps * len(rows)}), flush=True)
 
 
-def run_mixed(args, local):
+def run_mixed(args, local, kind="vamana"):
     """100,000 queries with Ls log-uniform in [10, 500] and k in {10, 50, 100}: one batched
-    launch (CUDA graph) against the plain kernel launched once per distinct (Ls, k)."""
+    launch (a CUDA graph on the Vamana graph) against the plain kernel launched once per
+    distinct (Ls, k); kind "hnsw": the same on the HNSW model (the batched launch is not
+    captured: beams above 256 use the epoch-tagged filter)."""
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     pgb = ge.load_package()
     nq = 100_000
-    base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana", nq)
+    if kind == "hnsw":
+        base, h = load_hnsw(pgb)
+        queries = rank_queries(0, nq)
+        index = pgb.Index.hnsw(base, h, device=local)
+    else:
+        base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana", nq)
+        index = pgb.Index.flat(base, graph, device=local)
     rng = np.random.default_rng(0)
     ls = np.rint(np.exp(rng.uniform(np.log(10), np.log(500), nq))).astype(np.uint32)
     ks = rng.choice(np.array([10, 50, 100], np.uint32), nq)
     max_k = 100
-    index = pgb.Index.flat(base, graph, device=local)
     q = torch.from_numpy(queries.view(np.uint8)).to(dev)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
@@ -841,10 +852,13 @@ def run_mixed(args, local):
     b.plan(ls, ks)
     ids, d, st = b.outputs(dev)
     tuned = b.tune(q, ids, d, st)
-    b.capture(q, ids, d, st)
     flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
     steps = max(3, args.steps // 20)
-    tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, 2, flush)
+    if kind == "hnsw":
+        tb = _timed_events(torch, stream, lambda: b.search(q, ids, d, st, sp), steps, 2, flush)
+    else:
+        b.capture(q, ids, d, st)
+        tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, 2, flush)
     # plain: the drop-in prepares one searcher per distinct (Ls, k) and launches it on
     # that group's queries; preparing and releasing are outside the timed launches
     groups = {}
@@ -871,8 +885,9 @@ def run_mixed(args, local):
         "unit": "queries/s", "n_gpus": 1, "steps": steps, "warmup": 2,
         "ms_per_step": sum(tb) / len(tb), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-        "config": {"workload": "1M int8 d=100 Vamana R64, 100000 queries, Ls log-uniform [10,500], "
-                               "k in {10,50,100}", "batched_qps": qb, "plain_qps": qp,
+        "config": {"workload": "1M int8 d=100 %s, 100000 queries, Ls log-uniform [10,500], "
+                               "k in {10,50,100}" % ("HNSW M32 efc128" if kind == "hnsw" else "Vamana R64"),
+                   "batched_qps": qb, "plain_qps": qp,
                    "plain_launches_per_step": len(plain), "batched_over_plain": qb / qp,
                    "plain_timing": "sum of per-group launch times (events), L2 warm",
                    "identical_neighbours": bool(same), "batched_config": tuned,

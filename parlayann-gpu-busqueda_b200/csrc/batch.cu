@@ -1,4 +1,4 @@
-// batch.cu -- pgb_batch_*: the batched persistent form of the flat-graph search.
+// batch.cu -- pgb_batch_*: the batched persistent form of the flat-graph and HNSW search.
 //
 // plan   : host step, per-query (Ls, k) -> longest-beam-first work order on the device
 // search : cudaMemsetAsync(counter) + one persistent launch (capturable); a plan whose
@@ -6,6 +6,8 @@
 // tune   : times candidate (warps per block, filter / visited placement) on the planned
 //          queries and keeps the fastest; every candidate returns identical neighbours,
 //          because all of them run the same per-query code (flat_query)
+// An HNSW index runs the HNSW kernel with each query at its own (Ls, k), its tables sized
+// for max_beam; it has a single launch shape, so tune only times it.
 #include <algorithm>
 #include <numeric>
 #include <string>
@@ -13,6 +15,7 @@
 
 #include "errors.h"
 #include "index.h"
+#include "search_hnsw.h"
 #include "search_plan.h"
 #include "searcher.h"
 
@@ -20,6 +23,8 @@ struct pgb_batch {
     pgb_index* index = nullptr;
     pgb_batch_options opt{};
     pgb::FlatPlan plan{};
+    bool hnsw = false;
+    pgb::HnswState hs{};  // HNSW index: the searcher state, prepared for max_beam
     float tuned_ms = 0.f;
     uint32_t* gfilter = nullptr;
     uint64_t gfilter_words = 0;   // allocated words
@@ -96,6 +101,13 @@ void drop_graph(pgb_batch* b) {
 pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_t qstride,
                    uint32_t* ids, int32_t* dists, pgb_query_stats* stats, cudaStream_t st) {
     const pgb_index* ix = b->index;
+    if (b->hnsw) {
+        if (b->uniform_ls)
+            return hnsw_launch_at(ix, b->hs, b->uniform_ls, b->uniform_k, b->opt.limit, queries, b->nq,
+                                  qstride, ids, dists, stats, b->opt.max_k, st);
+        return hnsw_launch_at(ix, b->hs, b->opt.max_beam, b->opt.max_k, b->opt.limit, queries, b->nq,
+                              qstride, ids, dists, stats, b->opt.max_k, st, b->d_ls, b->d_k, b->d_order);
+    }
     pgb_status s = cuda_status(cudaMemsetAsync(b->d_queue, 0, sizeof(uint32_t), st), "queue reset");
     if (s != PGB_OK) return s;
     FlatArgs A{};
@@ -153,7 +165,6 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
     if (!out) return fail(PGB_ERR_BAD_ARG, "null output handle");
     *out = nullptr;
     if (!ix || !opt) return fail(PGB_ERR_BAD_ARG, "null index or options");
-    if (ix->is_hnsw) return fail(PGB_ERR_BAD_ARG, "the batched form serves flat graphs");
     if (opt->max_queries == 0 || opt->max_beam == 0 || opt->max_beam > PGB_MAX_BEAM ||
         opt->max_k == 0 || opt->max_k > PGB_MAX_K || !(opt->cut > 0))
         return fail(PGB_ERR_BAD_ARG, "bad max_queries / max_beam / max_k / cut");
@@ -164,11 +175,18 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
     pgb_batch* b = new pgb_batch();
     b->index = ix;
     b->opt = *opt;
+    b->hnsw = ix->is_hnsw;
     pgb_status s;
     const size_t nq = opt->max_queries;
-    if ((s = make_plan(b, (int)opt->warps_per_block, (int)opt->filter_placement,
-                       (int)opt->visited_placement, b->plan)) != PGB_OK ||
-        (s = ensure_scratch(b, b->plan)) != PGB_OK ||
+    pgb_query_params hp{};
+    hp.k = opt->max_k;
+    hp.beam_size = opt->max_beam;
+    hp.cut = opt->cut;
+    hp.limit = opt->limit;
+    if ((s = b->hnsw ? hnsw_prepare(ix, hp, b->hs)
+                     : make_plan(b, (int)opt->warps_per_block, (int)opt->filter_placement,
+                                 (int)opt->visited_placement, b->plan)) != PGB_OK ||
+        (!b->hnsw && (s = ensure_scratch(b, b->plan)) != PGB_OK) ||
         (s = cuda_status(cudaMalloc(&b->d_ls, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_k, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_order, 4 * nq), "batch arrays")) != PGB_OK ||
@@ -268,6 +286,28 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    if (b->hnsw) {
+        // one launch shape: time it (warm-up, then the mean of two)
+        float ms = 0.f, t = 0.f;
+        s = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
+        for (int r = 0; r < 2 && s == PGB_OK; r++) {
+            cudaEventRecord(e0, st);
+            s = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
+            cudaEventRecord(e1, st);
+            if (s == PGB_OK && cudaEventSynchronize(e1) == cudaSuccess) {
+                cudaEventElapsedTime(&t, e0, e1);
+                ms += t;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        const cudaError_t e = cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+        if (s != PGB_OK) return s;
+        if (e != cudaSuccess) return cuda_status(e, "tune");
+        b->tuned_ms = ms / 2;
+        return PGB_OK;
+    }
     const int wpbs[] = {1, 2, 4};
     const int fpls[] = {1, 2};
     const int vpls[] = {1, 2};
@@ -312,6 +352,15 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
 
 pgb_status pgb_batch_get_config(const pgb_batch* b, pgb_batch_config* out) {
     if (!b || !out) return fail(PGB_ERR_BAD_ARG, "null argument");
+    if (b->hnsw) {
+        out->warps_per_block = (uint32_t)b->hs.warps_per_block;
+        out->blocks = (uint32_t)b->hs.blocks;
+        out->filter_in_shared = b->hs.fmode == 0 ? 1u : 0u;
+        out->visited_in_shared = 1u;  // is_inw is the workset, in shared memory
+        out->shared_bytes_per_warp = b->hs.warp_bytes;
+        out->tuned_ms = b->tuned_ms;
+        return PGB_OK;
+    }
     out->warps_per_block = (uint32_t)b->plan.warps_per_block;
     out->blocks = (uint32_t)b->plan.blocks;
     out->filter_in_shared = b->plan.sfilt ? 1u : 0u;
@@ -325,6 +374,10 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
                              int32_t* dists, pgb_query_stats* stats) {
     pgb_status s = check_call(b, queries, qstride, ids, dists);
     if (s != PGB_OK) return s;
+    // HNSW beams above 256 use a global (epoch, id) filter whose epochs advance on every
+    // launch; a replayed graph would repeat them and see the last replay's entries
+    if (b->hnsw && b->hs.fmode == 2)
+        return fail(PGB_ERR_BAD_ARG, "graph capture on HNSW needs max_beam <= 256");
     DeviceGuard guard(b->index->device);
     if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
     drop_graph(b);
@@ -365,6 +418,7 @@ pgb_status pgb_batch_destroy(pgb_batch* b) {
     if (!b) return PGB_OK;
     DeviceGuard guard(b->index ? b->index->device : 0);
     drop_graph(b);
+    hnsw_release(b->hs);
     cudaFree(b->gfilter);
     cudaFree(b->gvisited);
     cudaFree(b->d_ls);

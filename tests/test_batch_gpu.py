@@ -134,3 +134,50 @@ def test_batch_host_path_matches_device(pgb, oracle, golden, gpu):
     assert_same("ids", ids, oid)
     assert_same("dists", dists, od)
     assert_same("comps", stats[:, 0], oc)
+
+
+@pytest.mark.parametrize("max_beam", [160, 300])
+def test_batch_hnsw_mixed_beams_match_oracle(pgb, oracle, golden, gpu, max_beam):
+    """HNSW in the batched form: each query at its own (Ls, k) in one launch of the HNSW
+    kernel, tables sized for max_beam (300: the (epoch, id) global filter); the answer of
+    every query, its distance count and its flags are the oracle's for its (Ls, k). A
+    captured graph replays to the same answer (beams up to 256 only)."""
+    import torch
+    base, queries = golden.vectors_for("hnsw")
+    h = golden.hnsw["hnsw"]
+    rng = np.random.default_rng(3)
+    nq = len(queries)
+    ls = rng.choice([10, 25, 50, 100, max_beam], size=nq).astype(np.uint32)
+    ks = rng.choice([10, 20], size=nq).astype(np.uint32)
+    index = pgb.Index.hnsw(base, h)
+    b = pgb.Batch(index, nq, max_beam=max_beam, max_k=20)
+    b.plan(ls, ks)
+    q = torch.from_numpy(queries.view(np.uint8)).cuda()
+    ids, dists, stats = b.outputs(q.device)
+    b.search(q, ids, dists, stats)
+    torch.cuda.synchronize()
+    got_i = ids.cpu().numpy().view(np.uint32)
+    got_d = dists.cpu().numpy()
+    st = stats.cpu().numpy()
+    for qi in range(nq):
+        k = int(ks[qi])
+        oi, od, oc, oe, of = oracle.hnsw_search(base, h, queries[qi:qi + 1], k, int(ls[qi]))
+        assert_same(f"q{qi} ids", got_i[qi, :k], oi[0])
+        assert_same(f"q{qi} dists", got_d[qi, :k], od[0])
+        assert_same(f"q{qi} comps/exps/flags", st[qi, :3], [oc[0], oe[0], of[0]])
+    cfg = b.tune(q, ids, dists, stats)
+    assert cfg["tuned_ms"] > 0
+    if max_beam <= 256:
+        b.capture(q, ids, dists, stats)
+        for _ in range(2):
+            ids.fill_(0)
+            b.replay()
+            torch.cuda.synchronize()
+            rep = ids.cpu().numpy().view(np.uint32)
+            for qi in range(nq):
+                assert_same(f"replay q{qi}", rep[qi, :ks[qi]], got_i[qi, :ks[qi]])
+    else:
+        with pytest.raises(pgb.PgbError, match="256"):
+            b.capture(q, ids, dists, stats)
+    b.close()
+    index.close()
