@@ -197,6 +197,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), or None."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -535,9 +546,15 @@ def main():
             ts.append(time.perf_counter() - t)
         assert np.array_equal(oid, p_ids[:sample].cpu().numpy().view(np.uint32)), \
             "CUDA result differs from the CPU restatement"
+        # the same restatement on one thread, on the first 1,024 of the sample
+        q1 = np.ascontiguousarray(queries[:1024])
+        t = time.perf_counter()
+        oracle.flat_search(base, graph.degrees, graph.edges, q1, K, Ls, threads=1)
+        one = len(q1) / (time.perf_counter() - t)
         cpu_baseline = {"value": sample / min(ts), "unit": "queries/s", "cores": threads,
                         "kind": "port",
-                        "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}, best of 2"}
+                        "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}, best of 2",
+                        "one_thread_qps": one, "cpu_model": cpu_model()}
 
     if rank == 0:
         line = {

@@ -78,3 +78,42 @@ def test_degree_limit(pgb, oracle, golden, gpu, deg_lim):
     assert_same("ids", ids, oid)
     assert_same("dists", dists, od)
     assert_same("comps", st[:, 0], oc)
+
+
+def test_concurrent_searchers_share_an_index(pgb, golden, gpu):
+    """The threading contract: an index is read-only once created, so several host threads
+    may search it at once, each through its own searcher (own stream, own scratch). Four
+    threads on a flat and an HNSW index, at different beams, five rounds each: every round
+    returns the single-thread answer."""
+    import threading
+    base, queries = golden.vectors_for("vamana")
+    flat = pgb.Index.flat(base, golden.graphs["vamana"])
+    hnsw = pgb.Index.hnsw(base, golden.hnsw["hnsw"])
+    cfgs = [(flat, 20, 10), (flat, 64, 50), (hnsw, 50, 10), (hnsw, 300, 20)]
+    expect = []
+    for ix, Ls, k in cfgs:
+        s = pgb.Searcher(ix, len(queries), pgb.QueryParams(k=k, beam_size=Ls))
+        expect.append(s.search(queries))
+        s.liberar()
+    bad = []
+
+    def worker(i):
+        ix, Ls, k = cfgs[i]
+        s = pgb.Searcher(ix, len(queries), pgb.QueryParams(k=k, beam_size=Ls))
+        try:
+            for r in range(5):
+                ids, dists, st = s.search(queries)
+                if not (np.array_equal(ids, expect[i][0]) and np.array_equal(dists, expect[i][1])
+                        and np.array_equal(st, expect[i][2])):
+                    bad.append((i, r))
+        finally:
+            s.liberar()
+
+    threads = [threading.Thread(target=worker, args=(i,)) for i in range(len(cfgs))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not bad, bad
+    flat.close()
+    hnsw.close()
