@@ -538,9 +538,10 @@ def main():
         sample = 8192
         qs = np.ascontiguousarray(queries[:sample])
         threads = os.cpu_count() or 1
+        # the reference's protocol: one warm-up, then the best of 5 (comparacion1.cu:76-101)
         oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls, threads=threads)
         ts = []
-        for _ in range(2):
+        for _ in range(5):
             t = time.perf_counter()
             oid = oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls, threads=threads)[0]
             ts.append(time.perf_counter() - t)
@@ -553,7 +554,7 @@ def main():
         one = len(q1) / (time.perf_counter() - t)
         cpu_baseline = {"value": sample / min(ts), "unit": "queries/s", "cores": threads,
                         "kind": "port",
-                        "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}, best of 2",
+                        "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}, best of 5",
                         "one_thread_qps": one, "cpu_model": cpu_model()}
 
     if rank == 0:
