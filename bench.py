@@ -584,6 +584,8 @@ def main():
             "e2e": {"value": qps_e2e, "unit": "queries/s", "api": "pgb_batch_search_host",
                     "h2d_bytes_per_step": int(queries.nbytes),
                     "d2h_bytes_per_step": int(2 * 4 * N_QUERIES * K),
+                    "transfer": "pinned host buffers: the launch reads the queries from and "
+                                "writes ids / dists to host memory over the bus",
                     "identical_neighbours": e2e_ok},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,

@@ -213,7 +213,9 @@ pgb_status pgb_batch_search(pgb_batch* b, const void* queries, uint32_t query_st
                             uint32_t* ids, int32_t* dists, pgb_query_stats* stats,
                             void* stream);
 /* Same launch from and to HOST memory, synchronous: upload of the planned queries,
- * one launch, download of ids / dists / stats (stats may be NULL); row stride max_k. */
+ * one launch, download of ids / dists / stats (stats may be NULL); row stride max_k.
+ * When every buffer is page-locked (cudaHostAlloc / cudaHostRegister / torch
+ * pin_memory), the launch reads and writes them directly and no staging copy is made. */
 pgb_status pgb_batch_search_host(pgb_batch* b, const void* queries, uint32_t query_stride,
                                  uint32_t* ids, int32_t* dists, pgb_query_stats* stats);
 /* Autotuner: times the candidate launch shapes and table placements on the planned

@@ -145,6 +145,18 @@ pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_
     return launch_flat(P, A, st);
 }
 
+// the device address of page-locked host memory (the kernel reads and writes it over the
+// bus, no staging copy), or null for pageable or device memory
+void* pinned_device_ptr(const void* p) {
+    if (!p) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 pgb_status check_call(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
                       int32_t* dists) {
     if (!b) return fail(PGB_ERR_BAD_ARG, "null batch");
@@ -254,6 +266,18 @@ pgb_status pgb_batch_search_host(pgb_batch* b, const void* queries, uint32_t qst
     const pgb_index* ix = b->index;
     const size_t nq = b->nq, row = 4ull * b->opt.max_k;
     cudaStream_t st = b->stream;
+    // page-locked host buffers: one launch reads the queries and writes the results
+    // through them, so the transfers overlap the search instead of bracketing it
+    void* pq = pinned_device_ptr(queries);
+    void* pi = pinned_device_ptr(ids);
+    void* pd = pinned_device_ptr(dists);
+    void* ps = stats ? pinned_device_ptr(stats) : nullptr;
+    if (pq && pi && pd && (!stats || ps)) {
+        if ((s = enqueue(b, b->plan, pq, qstride, static_cast<uint32_t*>(pi), static_cast<int32_t*>(pd),
+                         static_cast<pgb_query_stats*>(ps), st)) != PGB_OK)
+            return s;
+        return cuda_status(cudaStreamSynchronize(st), "batch search");
+    }
     cudaError_t ce = (qstride == ix->dim)
                          ? cudaMemcpyAsync(b->q_dev, queries, nq * ix->dim, cudaMemcpyHostToDevice, st)
                          : cudaMemcpy2DAsync(b->q_dev, ix->dim, queries, qstride, ix->dim, nq,

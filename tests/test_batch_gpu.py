@@ -181,3 +181,34 @@ def test_batch_hnsw_mixed_beams_match_oracle(pgb, oracle, golden, gpu, max_beam)
             b.capture(q, ids, dists, stats)
     b.close()
     index.close()
+
+
+@pytest.mark.parametrize("kind", ["flat", "hnsw"])
+def test_batch_host_path_pinned_buffers(pgb, golden, gpu, kind):
+    """Page-locked host buffers are read and written by the launch itself; pageable ones
+    go through staging copies. Both give the device path's answers."""
+    import torch
+    base, queries = golden.vectors_for("vamana")
+    index = (pgb.Index.flat(base, golden.graphs["vamana"]) if kind == "flat"
+             else pgb.Index.hnsw(base, golden.hnsw["hnsw"]))
+    nq = len(queries)
+    rng = np.random.default_rng(7)
+    ls = rng.choice([20, 40, 64], size=nq).astype(np.uint32)
+    ks = rng.choice([5, 10], size=nq).astype(np.uint32)
+    b = pgb.Batch(index, nq, max_beam=64, max_k=10)
+    b.plan(ls, ks)
+    i0, d0, s0 = b.search_host(queries)  # pageable numpy buffers
+    q = torch.from_numpy(queries.view(np.uint8)).pin_memory()
+    ids = torch.full((nq, 10), -1, dtype=torch.int32).pin_memory()
+    dists = torch.full((nq, 10), -1, dtype=torch.int32).pin_memory()
+    st = torch.zeros((nq, 4), dtype=torch.int32).pin_memory()
+    for _ in range(2):
+        b.search_host(q, ids, dists, st)
+        gi = ids.numpy().view(np.uint32)
+        for qi in range(nq):
+            k = int(ks[qi])
+            assert_same(f"ids q{qi}", gi[qi, :k], i0[qi, :k])
+            assert_same(f"dists q{qi}", dists.numpy()[qi, :k], d0[qi, :k])
+        assert_same("stats", st.numpy()[:, :3], s0[:, :3])
+    b.close()
+    index.close()
