@@ -147,7 +147,8 @@ pgb_status pgb_searcher_search(pgb_searcher* s, const void* queries, uint32_t nq
                                uint32_t query_stride, uint32_t* ids, int32_t* dists,
                                pgb_query_stats* stats, void* stream);
 /* Same search from and to HOST memory, synchronous: copies the queries in, searches,
- * copies ids / dists / stats (stats may be NULL) out. */
+ * copies ids / dists / stats (stats may be NULL) out. When every buffer is page-locked,
+ * the launch reads and writes them directly and no staging copy is made. */
 pgb_status pgb_searcher_search_host(pgb_searcher* s, const void* queries, uint32_t nq,
                                     uint32_t query_stride, uint32_t* ids, int32_t* dists,
                                     pgb_query_stats* stats);

@@ -145,18 +145,6 @@ pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_
     return launch_flat(P, A, st);
 }
 
-// the device address of page-locked host memory (the kernel reads and writes it over the
-// bus, no staging copy), or null for pageable or device memory
-void* pinned_device_ptr(const void* p) {
-    if (!p) return nullptr;
-    cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
-}
-
 pgb_status check_call(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,
                       int32_t* dists) {
     if (!b) return fail(PGB_ERR_BAD_ARG, "null batch");

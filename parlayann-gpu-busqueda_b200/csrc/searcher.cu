@@ -28,6 +28,16 @@ pgb_status check_params(const pgb_index* ix, const pgb_query_params* p) {
     return PGB_OK;
 }
 
+void* pinned_device_ptr(const void* p) {
+    if (!p) return nullptr;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
 }  // namespace pgb
 
 using namespace pgb;
@@ -145,6 +155,19 @@ pgb_status pgb_searcher_search_host(pgb_searcher* S, const void* queries, uint32
     const size_t k = S->params.k;
     cudaStream_t st = S->stream;
     pgb_status s;
+    // page-locked host buffers: the launch reads the queries (at their stride) and writes
+    // the results through them, so the transfers overlap the search
+    void* pq = pinned_device_ptr(queries);
+    void* pi = pinned_device_ptr(ids);
+    void* pd = pinned_device_ptr(dists);
+    void* ps = stats ? pinned_device_ptr(stats) : nullptr;
+    if (pq && pi && pd && (!stats || ps)) {
+        if ((s = pgb_searcher_search(S, pq, nq, query_stride, static_cast<uint32_t*>(pi),
+                                     static_cast<int32_t*>(pd), static_cast<pgb_query_stats*>(ps),
+                                     st)) != PGB_OK)
+            return s;
+        return cuda_status(cudaStreamSynchronize(st), "search");
+    }
     // queries packed to dim bytes on the way in (one linear copy when already packed)
     cudaError_t ce =
         (query_stride == ix->dim)

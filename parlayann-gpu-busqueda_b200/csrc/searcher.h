@@ -26,4 +26,7 @@ struct pgb_searcher {
 namespace pgb {
 pgb_status cuda_status(cudaError_t e, const char* what);
 pgb_status check_params(const pgb_index* ix, const pgb_query_params* p);
+// the device address of page-locked host memory (a kernel reads and writes it over the
+// bus, no staging copy), or null for pageable or device memory
+void* pinned_device_ptr(const void* p);
 }  // namespace pgb

@@ -117,3 +117,30 @@ def test_concurrent_searchers_share_an_index(pgb, golden, gpu):
     assert not bad, bad
     flat.close()
     hnsw.close()
+
+
+@pytest.mark.parametrize("kind", ["flat", "hnsw"])
+def test_searcher_host_path_pinned_buffers(pgb, golden, gpu, kind):
+    """pgb_searcher_search_host with page-locked buffers: the launch reads the queries (at
+    their stride) and writes the results through them; the answers are those of the
+    staged path."""
+    import torch
+    base, queries = golden.vectors_for("vamana")
+    index = (pgb.Index.flat(base, golden.graphs["vamana"]) if kind == "flat"
+             else pgb.Index.hnsw(base, golden.hnsw["hnsw"]))
+    nq, k = len(queries), 10
+    s = pgb.Searcher(index, nq, pgb.QueryParams(k=k, beam_size=50))
+    want_i, want_d, want_s = s.search(queries)  # pageable numpy: staging copies
+    wide = torch.zeros((nq, 112), dtype=torch.uint8).pin_memory()  # rows 112 bytes apart
+    wide[:, :queries.shape[1]] = torch.from_numpy(queries.view(np.uint8))
+    ids = torch.full((nq, k), -1, dtype=torch.int32).pin_memory()
+    dists = torch.full((nq, k), -1, dtype=torch.int32).pin_memory()
+    st = torch.zeros((nq, 4), dtype=torch.int32).pin_memory()
+    lib = pgb._native.lib
+    pgb._native.check(lib.pgb_searcher_search_host(s._h, wide.data_ptr(), nq, 112, ids.data_ptr(),
+                                                   dists.data_ptr(), st.data_ptr()))
+    assert_same("ids", ids.numpy().view(np.uint32), want_i)
+    assert_same("dists", dists.numpy(), want_d)
+    assert_same("stats", st.numpy()[:, :3], want_s[:, :3])
+    s.liberar()
+    index.close()
