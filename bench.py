@@ -371,7 +371,7 @@ def main():
     ap.add_argument("--profile-ls", type=int, default=40)
     ap.add_argument("--workload", default="vamana",
                     choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "mixed_hnsw", "serving",
-                             "serving_hnsw", "c4", "build"],
+                             "serving_hnsw", "c4", "build", "codes"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
                          "mixed / mixed_hnsw: 100k queries of uneven Ls and k in one launch "
@@ -379,7 +379,8 @@ def main():
                          "serving_hnsw: Poisson bursts through the request loop on the Vamana "
                          "graph / the HNSW model; c4: 10M uint8 d=128 Vamana, 100k queries, "
                          "Ls 20/50/100/200; build: GPU vs CPU Vamana, HNSW and HCNNG "
-                         "construction on the 1M base")
+                         "construction on the 1M base; codes: 4-bit code rows + exact re-rank "
+                         "vs vector rows, plain kernel, 1M Vamana")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.profile:
@@ -389,11 +390,11 @@ def main():
             run_profile(args, local)
         return
     if args.workload in ("hnsw", "mixed", "mixed_hnsw", "serving", "serving_hnsw", "c4",
-                         "build") and args.impl == "ours":
+                         "build", "codes") and args.impl == "ours":
         {"hnsw": run_hnsw, "mixed": run_mixed, "mixed_hnsw": lambda a, lo: run_mixed(a, lo, "hnsw"),
          "serving": run_serving,
          "serving_hnsw": lambda a, lo: run_serving(a, lo, "hnsw"), "c4": run_c4,
-         "build": run_build}[args.workload](args, local)
+         "build": run_build, "codes": run_codes}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -679,6 +680,81 @@ def run_hnsw(args, local):
                      "frac": achieved / peak, "traffic": None, "peak_source": kind,
                      "kernel": "hnsw_kernel"},
         "gpu_launches": args.steps}), flush=True)
+
+
+def run_codes(args, local):
+    """Compressed rows on the 1M Vamana workload: the plain kernel over 4-bit code rows
+    (64 bytes per point; the 64 MB of codes fit in L2) with an exact re-rank of the whole
+    final frontier (rerank = Ls), against the plain kernel over the 128-byte vector rows,
+    each at its smallest sweep beam reaching recall@10 >= 0.90."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
+    base, queries, graph = load_workload(pgb, 0, lambda: None)
+    gt_ids, gt_d = ground_truth(base, queries, 0, local)
+    index = pgb.Index.flat(base, graph, device=local)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    index.compress()
+    compress_s = time.time() - t0
+    step, off, _ = index.codes(rows=False)
+    q = torch.from_numpy(queries.view(np.uint8)).to(dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+    gs = (int(index.info.max_degree) + 31) // 32 * 32
+    peak, kind = measured_peaks()
+    out = {}
+    for name, rr in (("vector_rows", False), ("code_rows", True)):
+        sweep, Ls = [], None
+        for ls in LS_SWEEP:
+            s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=ls), rerank=ls if rr else 0)
+            ids, _, _ = s.search_device(q, stream.cuda_stream)
+            torch.cuda.synchronize()
+            rec = pgb.recall(gt_ids, gt_d, ids.cpu().numpy().view(np.uint32), K)
+            sweep.append([ls, round(rec, 5)])
+            s.liberar()
+            if rec >= TARGET_RECALL and Ls is None:
+                Ls = ls
+            if Ls is not None and ls >= 2 * Ls:
+                break
+        Ls = Ls or LS_SWEEP[-1]
+        s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=Ls), rerank=Ls if rr else 0)
+        ids = torch.empty((N_QUERIES, K), dtype=torch.int32, device=dev)
+        d = torch.empty_like(ids)
+        st = torch.empty((N_QUERIES, 4), dtype=torch.int32, device=dev)
+        t = _timed_events(torch, stream, lambda: s.lanzar(q, ids, d, st, stream.cuda_stream),
+                          args.steps, args.warmup, flush)
+        stn = st.cpu().numpy().astype(np.int64)
+        ms = sum(t) / len(t)
+        row_b = 64 if rr else 128
+        # gathered rows + adjacency rows (+ the re-rank's vector rows)
+        bytes_launch = float(row_b * stn[:, 0].sum() + 4 * gs * stn[:, 1].sum()
+                             + (128 * Ls * N_QUERIES if rr else 0))
+        achieved = bytes_launch / (ms / 1e3) / 1e9
+        out[name] = {"Ls": Ls, "rerank": Ls if rr else None, "qps": N_QUERIES / (ms / 1e3),
+                     "ms_per_step": ms, "recall_at_10": dict((a, b) for a, b in sweep)[Ls],
+                     "sweep_recall": sweep, "comps_per_query": float(stn[:, 0].mean()),
+                     "expansions_per_query": float(stn[:, 1].mean()),
+                     "algorithmic_gb_per_s": achieved, "frac_of_hbm_peak": achieved / peak}
+        s.liberar()
+    c, v = out["code_rows"], out["vector_rows"]
+    print(json.dumps({
+        "metric": "QPS @ recall@10=0.90, plain kernel over 4-bit code rows + exact re-rank, 1 B200",
+        "value": c["qps"], "unit": "queries/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": c["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8 (4-bit codes)", "data": "synthetic",
+        "config": {"workload": "1M int8 d=100 Gaussian mixture, Vamana R64 L128 alpha1.2, "
+                               "29316 queries, k=10",
+                   "code_step": step, "compress_s": compress_s,
+                   "l2": "flushed (512 MiB write) before every timed step",
+                   "code_rows": c, "vector_rows": v,
+                   "codes_over_vectors": c["qps"] / v["qps"]},
+        "roofline": {"bound": "hbm", "achieved": c["algorithmic_gb_per_s"], "peak": peak,
+                     "unit": "GB/s", "frac": c["frac_of_hbm_peak"], "traffic": None,
+                     "peak_source": kind, "kernel": "flat_plain_kernel (code rows) + rerank_kernel"},
+        "gpu_launches": 2 * args.steps}), flush=True)
 
 
 def run_build(args, local):

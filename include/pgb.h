@@ -155,6 +155,32 @@ pgb_status pgb_searcher_search_host(pgb_searcher* s, const void* queries, uint32
 /* liberar */
 pgb_status pgb_searcher_destroy(pgb_searcher* s);
 
+/* ---- compressed rows (no counterpart in the reference) -----------------------------
+ * 4-bit codes, 64 bytes per point next to the 128-byte vector rows: the compressed form
+ * the reference's paper points to (BANG's PQ, paper/paper.tex:134-136), here as a scalar
+ * code whose distances stay exact integers. Dimension d of a point is stored as a code c
+ * in 0..15 standing for v = step * c + offsets[d] (c = round half up of (x - offsets[d]) /
+ * step, clamped), so a search over the codes is exactly the search over the
+ * reconstructed vectors v. Flat graphs with dim <= 120 only.
+ * pgb_index_compress: step == 0 chooses step (1..17) and offsets from per-dimension
+ * histograms, minimising the total squared reconstruction error (ties: smaller step, then
+ * smaller offset); otherwise the given step and offsets[dim] are used (each v must stay
+ * inside the element's range). Replaces earlier codes of the index. */
+pgb_status pgb_index_compress(pgb_index* index, int32_t step, const int32_t* offsets);
+/* The index's step, offsets[dim] (may be NULL) and code rows (n x 64 bytes into host
+ * memory; may be NULL). */
+pgb_status pgb_index_get_codes(const pgb_index* index, int32_t* step, int32_t* offsets,
+                               uint8_t* codes);
+/* A searcher over the code rows (plain schedule): ParlayANN's beam search with params on
+ * the reconstructed vectors keeps the first `rerank` entries of each final frontier
+ * (k <= rerank <= beam_size), which are then re-ranked by their exact distance to the
+ * vector rows (ties by id); ids / dists receive the k best. pgb_searcher_search and
+ * pgb_searcher_search_host run it; stats are those of the search over the codes, as if
+ * it returned `rerank` neighbours (PGB_FLAG_SHORT: fewer than `rerank` entries). */
+pgb_status pgb_searcher_create_compressed(pgb_index* index, uint32_t max_queries,
+                                          const pgb_query_params* params, uint32_t rerank,
+                                          pgb_searcher** out);
+
 /* ---- plain search without device allocation (no counterpart in the reference) ------
  * For callers that may not allocate device memory at query time: cudaMalloc and cudaFree
  * can synchronise the whole device (stalling every other stream of a serving process),

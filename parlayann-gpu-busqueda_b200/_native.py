@@ -81,6 +81,10 @@ _sig("pgb_searcher_create", C.c_int, vp, u32, C.POINTER(QueryParams), C.POINTER(
 _sig("pgb_searcher_search", C.c_int, vp, vp, u32, u32, vp, vp, vp, vp)
 _sig("pgb_searcher_search_host", C.c_int, vp, vp, u32, u32, vp, vp, vp)
 _sig("pgb_searcher_destroy", C.c_int, vp)
+_sig("pgb_index_compress", C.c_int, vp, i32, vp)
+_sig("pgb_index_get_codes", C.c_int, vp, C.POINTER(i32), vp, vp)
+_sig("pgb_searcher_create_compressed", C.c_int, vp, u32, C.POINTER(QueryParams), u32,
+     C.POINTER(vp))
 _sig("pgb_search_flat_noalloc", C.c_int, vp, C.POINTER(QueryParams), vp, u32, u32, vp, vp, vp,
      vp)
 _sig("pgb_recall", C.c_double, vp, vp, u32, u32, vp, u32)

@@ -100,6 +100,42 @@ __device__ __forceinline__ int32_t partial_dot(const int4 p, const int4 q) {
 // 124..127; the query row has zeros there, so it drops out of every dot product.
 constexpr uint32_t kNormInRowMaxDim = 124;
 
+// Compressed rows: 4-bit codes, 64 bytes per row. Byte b of 32-bit word j of 16-byte
+// word c holds dimension 32c + 8j + b in its low nibble and 32c + 8j + 4 + b in its high
+// nibble (so the low nibbles pair with query word 8c + 2j, the high ones with 8c + 2j + 1,
+// and the query row keeps its natural byte order). Bytes 60..63 hold the squared norm of
+// the reconstructed row, which leaves room for 120 dimensions.
+constexpr int kCodeRowBytes = 64;
+constexpr uint32_t kCodeMaxDim = 120;
+
+// acc + dot of the four query bytes q (signed when Signed) with four unsigned bytes c
+template <bool Signed>
+__device__ __forceinline__ int32_t dp4a_qc(uint32_t q, uint32_t c, int32_t acc) {
+    int32_t d;
+    if (Signed)
+        asm("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(q), "r"(c), "r"(acc));
+    else
+        asm("dp4a.u32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(q), "r"(c), "r"(acc));
+    return d;
+}
+
+// dot of 16 code bytes (32 codes) with the 32 query bytes qa (the word's first 16
+// dimensions) and qb (the next 16). The high nibbles are used in place (16 x code); their
+// sum is a multiple of 16 and is divided by 16 at the end, exactly.
+template <bool Signed>
+__device__ __forceinline__ int32_t code_dot(const int4 v, const int4 qa, const int4 qb) {
+    constexpr uint32_t lo = 0x0F0F0F0Fu, hi = 0xF0F0F0F0u;
+    int32_t a = dp4a_qc<Signed>((uint32_t)qa.x, (uint32_t)v.x & lo, 0);
+    int32_t b = dp4a_qc<Signed>((uint32_t)qa.y, (uint32_t)v.x & hi, 0);
+    a = dp4a_qc<Signed>((uint32_t)qa.z, (uint32_t)v.y & lo, a);
+    b = dp4a_qc<Signed>((uint32_t)qa.w, (uint32_t)v.y & hi, b);
+    a = dp4a_qc<Signed>((uint32_t)qb.x, (uint32_t)v.z & lo, a);
+    b = dp4a_qc<Signed>((uint32_t)qb.y, (uint32_t)v.z & hi, b);
+    a = dp4a_qc<Signed>((uint32_t)qb.z, (uint32_t)v.w & lo, a);
+    b = dp4a_qc<Signed>((uint32_t)qb.w, (uint32_t)v.w & hi, b);
+    return a + (b >> 4);
+}
+
 template <bool Signed>
 __device__ __forceinline__ int32_t partial_sq(const int4 q) {
     if (Signed) {

@@ -152,6 +152,8 @@ void free_index(pgb_index* ix) {
     cudaFree(ix->upper_start);
     cudaFree(ix->node_point);
     if (ix->node_rows && ix->node_rows != ix->rows) cudaFree(ix->node_rows);
+    cudaFree(ix->codes);
+    cudaFree(ix->code_off);
     delete ix;
 }
 

@@ -40,6 +40,13 @@ struct pgb_index {
     uint32_t n_entries = 0;
     uint32_t top_level = 0;
     uint64_t device_bytes = 0;
+    // flat graphs, after pgb_index_compress: n x 64-byte 4-bit code rows; dimension d of a
+    // row is code_step * code + code_off_host[d] (code_off: the offsets as one 128-byte
+    // row of element values on the device)
+    uint8_t* codes = nullptr;
+    uint8_t* code_off = nullptr;
+    int32_t code_step = 0;
+    int32_t code_off_host[PGB_MAX_DIM] = {0};
 };
 
 namespace pgb {

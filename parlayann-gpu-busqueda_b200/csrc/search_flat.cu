@@ -63,7 +63,10 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     P.gfilter_words = P.sfilt ? 0u : fwords;
     P.gvisited_words = P.svis ? 0u : vwords;
     const uint32_t kfw = P.sfilt ? fwords : 0u;
-    P.kernel = pick(P.ch, P.batched ? FlatSchedule::kBatched : FlatSchedule::kPlain, P.is_signed, kfw);
+    if (rq.codes && rq.batched) return fail(PGB_ERR_BAD_ARG, "code rows are searched by the plain schedule only");
+    const FlatSchedule sched = P.batched ? FlatSchedule::kBatched
+                                         : (rq.codes ? FlatSchedule::kPlainCodes : FlatSchedule::kPlain);
+    P.kernel = pick(P.ch, sched, P.is_signed, kfw);
     if (P.batched) P.kernel_uniform = pick(P.ch, FlatSchedule::kBatchedUniform, P.is_signed, kfw);
     if (!P.kernel || (P.batched && !P.kernel_uniform))
         return fail(PGB_ERR_BAD_ARG, "no kernel for this filter size");

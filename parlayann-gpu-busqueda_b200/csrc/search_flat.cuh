@@ -152,8 +152,9 @@ __host__ __device__ constexpr FlatLayout make_flat_layout(uint32_t ls_cap, uint3
 }
 
 // plain: static query striding; batched: device work queue with per-query (Ls, k);
-// batched uniform: work queue, one (Ls, k) for the whole launch
-enum class FlatSchedule { kPlain, kBatched, kBatchedUniform };
+// batched uniform: work queue, one (Ls, k) for the whole launch; plain codes: the plain
+// schedule over 4-bit code rows
+enum class FlatSchedule { kPlain, kBatched, kBatchedUniform, kPlainCodes };
 
 struct FlatArgs {
     const uint8_t* rows;   // n x 128-byte vector rows
@@ -179,6 +180,10 @@ struct FlatArgs {
     uint32_t* gvisited;             // per-warp global visited tables when not in shared
     uint32_t gvisited_words;
     uint32_t* queue;                // batched: next-query counter
+    // code rows (kPlainCodes): rows holds n x 64-byte code rows, a dimension's value is
+    // code_step * code + its offset (code_off: one 128-byte row of element values)
+    int32_t code_step;
+    const uint8_t* code_off;
 };
 
 // ---- exact visited multiset (keys only; duplicates occupy several slots) ----------
@@ -369,6 +374,55 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
     __syncwarp();
 }
 
+// ---- distances over 4-bit code rows: 4 lanes per 64-byte row, 8*SLOTS rows in flight --
+// Lane c reads the row's 16-byte word c (dimensions 32c..32c+31) and pairs it with query
+// words 2c and 2c+1. With v = step * code + offset per dimension,
+//   ||q - v||^2 = (||q||^2 - 2 q.offset) - 2 step (q.code) + ||v||^2,
+// where qq carries the first term and ||v||^2 sits in bytes 60..63 (word 3's last int,
+// held by lane 3; the query is zero over those dimensions, so its codes add nothing).
+template <bool Signed, int SLOTS = PGB_DIST_SLOTS>
+__device__ __forceinline__ void code_row_distances(const uint8_t* __restrict__ codes,
+                                                   const uint32_t* ids, int32_t* out, int np,
+                                                   const int4* q4, const int32_t qq,
+                                                   int32_t step, int lane) {
+    const int grp = lane >> 2, c = lane & 3;
+    const int4 qa = q4[2 * c], qb = q4[2 * c + 1];
+    for (int base = 0; base < np; base += 8 * SLOTS) {
+        int4 v[SLOTS];
+#pragma unroll
+        for (int r = 0; r < SLOTS; r++) {
+            const int i = base + r * 8 + grp;
+            // slots past np re-read row ids[0], as in row_distances
+            v[r] = ldg16(codes + (size_t)ids[i < np ? i : 0] * kCodeRowBytes + c * 16);
+        }
+        int32_t t[SLOTS];
+#pragma unroll
+        for (int r = 0; r < SLOTS; r++)
+            t[r] = (c == 3 ? v[r].w : 0) - 2 * step * code_dot<Signed>(v[r], qa, qb);
+#pragma unroll
+        for (int off = 2; off > 0; off >>= 1)
+#pragma unroll
+            for (int r = 0; r < SLOTS; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 4);
+        if (c == 0) {
+#pragma unroll
+            for (int r = 0; r < SLOTS; r++) {
+                const int i = base + r * 8 + grp;
+                if (i < np) out[i] = qq + t[r];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// dot(q, o) of a zero-padded 128-byte query row with a 128-byte row o, on every lane
+template <bool Signed>
+__device__ __forceinline__ int32_t query_row_dot(const int4* q4, const uint8_t* o, int lane) {
+    int32_t s = partial_dot<Signed>(ldg16(o + 16 * (lane & 7)), q4[lane & 7]);
+#pragma unroll
+    for (int off = 4; off > 0; off >>= 1) s += __shfl_xor_sync(kFull, s, off, 8);
+    return s;
+}
+
 // ||q||^2 of a zero-padded 128-byte query row, on every lane
 template <bool Signed>
 __device__ __forceinline__ int32_t query_sq_norm(const int4* q4, int lane) {
@@ -385,7 +439,19 @@ __device__ __forceinline__ int32_t query_sq_norm(const int4* q4, int lane) {
 // gfilter. Offsets up to the frontier keys are compile-time constants (K); a shared
 // visited table sits after the frontier, at the plan's offset (A.L), which the host
 // computes with the same make_flat_layout.
-template <int CH, bool Signed, int FW>
+// C4: A.rows holds 4-bit code rows (kCodeRowBytes each) and distances are those of the
+// reconstructed vectors (code_row_distances); otherwise 128-byte vector rows.
+template <bool Signed, bool C4>
+__device__ __forceinline__ void pending_distances(const FlatArgs& A, const uint32_t* ids,
+                                                  int32_t* out, int np, const int4* q4,
+                                                  int32_t qq, bool nir, int lane) {
+    if constexpr (C4)
+        code_row_distances<Signed>(A.rows, ids, out, np, q4, qq, A.code_step, lane);
+    else
+        row_distances<Signed>(A.rows, ids, out, np, q4, qq, A.dim, nir, lane);
+}
+
+template <int CH, bool Signed, int FW, bool C4 = false>
 __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfilter,
                            uint32_t* gvisited, uint32_t q, uint32_t Ls, uint32_t k, int lane) {
     constexpr bool SFILT = FW > 0;
@@ -430,13 +496,14 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     }
     __syncwarp();
     const int4* q4 = reinterpret_cast<const int4*>(qwords);
-    const int32_t qq = query_sq_norm<Signed>(q4, lane);
+    int32_t qq = query_sq_norm<Signed>(q4, lane);
+    if constexpr (C4) qq -= 2 * query_row_dot<Signed>(q4, A.code_off, lane);
 
     // start point: F = {(d(q, start), start)}, one distance
     if (lane == 0) pend[0] = A.start;
     __syncwarp();
     const bool nir = A.norm_in_row != 0;
-    row_distances<Signed>(A.rows, pend, pdist, 1, q4, qq, A.dim, nir, lane);
+    pending_distances<Signed, C4>(A, pend, pdist, 1, q4, qq, nir, lane);
     if (lane == 0) {
         fkey[0] = pack_key(pdist[0], A.start);
         fvis[0] = 0;
@@ -566,7 +633,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         PGB_PROF_ADD(SEC_FILTER, tp);
 
         // ---- distances ------------------------------------------------------------
-        row_distances<Signed>(A.rows, pend, pdist, np, q4, qq, A.dim, nir, lane);
+        pending_distances<Signed, C4>(A, pend, pdist, np, q4, qq, nir, lane);
         PGB_PROF_ADD(SEC_DIST, tp);
 
         // ---- candidates under the cutoff, in arrival order ------------------------
@@ -744,7 +811,8 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         if (u >= 0 && key_id(fkey[u]) == pred) {
 #pragma unroll
             for (int t = 0; t < CH; t++)
-                if (apred[t] != kEmptyId) prefetch_row_l2(A.rows + (size_t)apred[t] * kRowBytes);
+                if (apred[t] != kEmptyId)
+                    prefetch_row_l2(A.rows + (size_t)apred[t] * (C4 ? kCodeRowBytes : kRowBytes));
         }
         __syncwarp();
         PGB_PROF_ADD(SEC_CUT_NEXT, tp);

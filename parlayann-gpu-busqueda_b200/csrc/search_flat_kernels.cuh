@@ -42,7 +42,8 @@ static __device__ unsigned long long g_section_cycles[NUM_SECTIONS];
 #define PGB_PROF_EXIT()
 #endif
 
-template <int CH, bool Signed, int FW>
+// C4: the rows are 4-bit code rows (schedule kPlainCodes)
+template <int CH, bool Signed, int FW, bool C4 = false>
 __global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_plain_kernel(FlatArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_plain_kernel(FlatArg
     uint32_t* gv = A.gvisited ? A.gvisited + (size_t)gw * A.gvisited_words : nullptr;
     PGB_PROF_ENTER();
     for (uint32_t q = gw; q < A.nq; q += total)
-        flat_query<CH, Signed, FW>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
+        flat_query<CH, Signed, FW, C4>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
     PGB_PROF_EXIT();
 }
 
@@ -92,6 +93,7 @@ void* flat_kernel_of(FlatSchedule sched) {
     switch (sched) {
         case FlatSchedule::kPlain: return (void*)flat_plain_kernel<CH, Signed, FW>;
         case FlatSchedule::kBatched: return (void*)flat_batched_kernel<CH, Signed, FW, false>;
+        case FlatSchedule::kPlainCodes: return (void*)flat_plain_kernel<CH, Signed, FW, true>;
         default: return (void*)flat_batched_kernel<CH, Signed, FW, true>;
     }
 }

@@ -15,6 +15,7 @@ struct FlatPlanRequest {
     uint32_t deg_lim = 32;         // adjacency entries read per row
     bool is_signed = true;
     bool batched = false;
+    bool codes = false;            // plain schedule over 4-bit code rows (not batched)
     int warps_per_block = 0;       // 0: default (4)
     int max_blocks_per_sm = 0;     // 0: as many as fit
     // table placement: the lossy filter is read on every neighbour and stays in shared

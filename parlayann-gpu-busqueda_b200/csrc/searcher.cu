@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <string>
 
+#include "codes.h"
 #include "errors.h"
 #include "index.h"
 #include "search_hnsw.h"
@@ -38,33 +39,45 @@ void* pinned_device_ptr(const void* p) {
     return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
 }
 
-}  // namespace pgb
+namespace {
 
-using namespace pgb;
-
-extern "C" {
-
-pgb_status pgb_searcher_create(pgb_index* ix, uint32_t max_queries,
-                               const pgb_query_params* params, pgb_searcher** out) {
+// rerank > 0: a search over the index's code rows keeping `rerank` candidates per query
+pgb_status create_searcher(pgb_index* ix, uint32_t max_queries, const pgb_query_params* params,
+                           uint32_t rerank, pgb_searcher** out) {
     if (!out) return fail(PGB_ERR_BAD_ARG, "null output handle");
     *out = nullptr;
     if (!ix || max_queries == 0) return fail(PGB_ERR_BAD_ARG, "null index or max_queries == 0");
     pgb_status s = check_params(ix, params);
     if (s != PGB_OK) return s;
+    if (rerank) {
+        if (ix->is_hnsw || !ix->codes) return fail(PGB_ERR_BAD_ARG, "index has no code rows (pgb_index_compress)");
+        if (rerank < params->k || rerank > params->beam_size)
+            return fail(PGB_ERR_BAD_ARG, "rerank outside k..beam_size");
+    }
     DeviceGuard guard(ix->device);
     if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
     pgb_searcher* S = new pgb_searcher();
     S->index = ix;
     S->params = *params;
     S->max_queries = max_queries;
+    S->codes = rerank > 0;
+    S->rerank = rerank;
     if (!ix->is_hnsw) {
         FlatPlanRequest rq;
         rq.max_ls = params->beam_size;
         rq.deg_lim = params->degree_limit ? std::min(params->degree_limit, ix->G) : ix->G;
         rq.is_signed = ix->elem == PGB_INT8;
         rq.batched = false;
+        rq.codes = S->codes;
         if ((s = plan_flat(rq, S->flat)) != PGB_OK) {
             delete S;
+            return s;
+        }
+        if (S->codes &&
+            ((s = cuda_status(cudaMalloc(&S->cand, 4ull * max_queries * rerank), "candidate ids")) != PGB_OK ||
+             (s = cuda_status(cudaMalloc(&S->cand_d, 4ull * max_queries * rerank), "candidate distances")) !=
+                 PGB_OK)) {
+            pgb_searcher_destroy(S);
             return s;
         }
         if (S->flat.gfilter_words &&
@@ -98,6 +111,25 @@ pgb_status pgb_searcher_create(pgb_index* ix, uint32_t max_queries,
     }
     *out = S;
     return PGB_OK;
+}
+
+}  // namespace
+}  // namespace pgb
+
+using namespace pgb;
+
+extern "C" {
+
+pgb_status pgb_searcher_create(pgb_index* ix, uint32_t max_queries,
+                               const pgb_query_params* params, pgb_searcher** out) {
+    return create_searcher(ix, max_queries, params, 0, out);
+}
+
+pgb_status pgb_searcher_create_compressed(pgb_index* ix, uint32_t max_queries,
+                                          const pgb_query_params* params, uint32_t rerank,
+                                          pgb_searcher** out) {
+    if (rerank == 0) return fail(PGB_ERR_BAD_ARG, "rerank == 0");
+    return create_searcher(ix, max_queries, params, rerank, out);
 }
 
 pgb_status pgb_searcher_search(pgb_searcher* S, const void* queries, uint32_t nq,
@@ -138,7 +170,19 @@ pgb_status pgb_searcher_search(pgb_searcher* S, const void* queries, uint32_t nq
     A.stats = stats;
     A.gfilter = S->gfilter;
     A.gvisited = S->gvisited;
-    return launch_flat(S->flat, A, st);
+    if (!S->codes) return launch_flat(S->flat, A, st);
+    // code rows: the search keeps the first `rerank` entries of each frontier, then the
+    // exact re-rank writes the caller's k
+    A.rows = ix->codes;
+    A.code_step = ix->code_step;
+    A.code_off = ix->code_off;
+    A.k = S->rerank;
+    A.out_stride = S->rerank;
+    A.ids = S->cand;
+    A.dists = S->cand_d;
+    pgb_status s = launch_flat(S->flat, A, st);
+    if (s != PGB_OK) return s;
+    return rerank_launch(ix, queries, nq, query_stride, S->cand, S->rerank, p.k, ids, dists, st);
 }
 
 pgb_status pgb_searcher_search_host(pgb_searcher* S, const void* queries, uint32_t nq,
@@ -197,6 +241,8 @@ pgb_status pgb_searcher_destroy(pgb_searcher* S) {
     if (S->stream) cudaStreamDestroy(S->stream);
     cudaFree(S->gfilter);
     cudaFree(S->gvisited);
+    cudaFree(S->cand);
+    cudaFree(S->cand_d);
     cudaFree(S->q_dev);
     cudaFree(S->ids_dev);
     cudaFree(S->dists_dev);

@@ -15,6 +15,12 @@ struct pgb_searcher {
     uint32_t* gfilter = nullptr;   // flat: per-warp filters when not in shared memory
     uint32_t* gvisited = nullptr;  // flat: per-warp visited tables when not in shared
     pgb::HnswState hnsw{};
+    // code rows (pgb_searcher_create_compressed): the search keeps `rerank` candidates per
+    // query in cand / cand_d, re-ranked exactly into the caller's k
+    bool codes = false;
+    uint32_t rerank = 0;
+    uint32_t* cand = nullptr;
+    int32_t* cand_d = nullptr;
     // host-memory path staging
     uint8_t* q_dev = nullptr;
     uint32_t* ids_dev = nullptr;

@@ -99,6 +99,23 @@ class Index:
     def handle(self):
         return self._h
 
+    def compress(self, step: int = 0, offsets=None) -> None:
+        """4-bit code rows next to the vectors (flat graphs, dim <= 120): dimension d is
+        stored as c in 0..15 standing for step * c + offsets[d]. step 0 chooses step and
+        offsets from the data (least squared reconstruction error)."""
+        off = None if offsets is None else np.ascontiguousarray(offsets, dtype=np.int32)
+        N.check(N.lib.pgb_index_compress(self._h, int(step), _ptr(off)))
+        self.info = N.IndexInfo()
+        N.check(N.lib.pgb_index_get_info(self._h, C.byref(self.info)))
+
+    def codes(self, rows: bool = True):
+        """(step, offsets int32 [dim], code rows uint8 [n, 64] or None)."""
+        step = C.c_int32()
+        off = np.zeros(self.info.dim, dtype=np.int32)
+        codes = np.empty((self.info.n_points, 64), dtype=np.uint8) if rows else None
+        N.check(N.lib.pgb_index_get_codes(self._h, C.byref(step), _ptr(off), _ptr(codes)))
+        return step.value, off, codes
+
     def close(self):
         if self._h:
             N.lib.pgb_index_destroy(self._h)
@@ -114,12 +131,19 @@ class Index:
 class Searcher:
     """BuscadorGPU / BuscadorHnsw: prepare once for (index, max queries, params)."""
 
-    def __init__(self, index: Index, max_queries: int, params: QueryParams):
+    def __init__(self, index: Index, max_queries: int, params: QueryParams, rerank: int = 0):
+        """rerank > 0: search the index's code rows (Index.compress) keeping `rerank`
+        candidates per query (k <= rerank <= beam_size), re-ranked exactly into k."""
         self.index, self.params, self.max_queries = index, params, max_queries
+        self.rerank = rerank
         self._cp = params.to_c()
         h = C.c_void_p()
-        N.check(N.lib.pgb_searcher_create(index.handle, max_queries, C.byref(self._cp),
-                                          C.byref(h)))
+        if rerank:
+            N.check(N.lib.pgb_searcher_create_compressed(index.handle, max_queries,
+                                                         C.byref(self._cp), rerank, C.byref(h)))
+        else:
+            N.check(N.lib.pgb_searcher_create(index.handle, max_queries, C.byref(self._cp),
+                                              C.byref(h)))
         self._h = h
 
     def lanzar(self, queries, ids, dists, stats=None, stream: int = 0, query_stride=None):
