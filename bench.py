@@ -724,20 +724,30 @@ def run_codes(args, local):
         ids = torch.empty((N_QUERIES, K), dtype=torch.int32, device=dev)
         d = torch.empty_like(ids)
         st = torch.empty((N_QUERIES, 4), dtype=torch.int32, device=dev)
-        t = _timed_events(torch, stream, lambda: s.lanzar(q, ids, d, st, stream.cuda_stream),
-                          args.steps, args.warmup, flush)
-        stn = st.cpu().numpy().astype(np.int64)
-        ms = sum(t) / len(t)
-        row_b = 64 if rr else 128
-        # gathered rows + adjacency rows (+ the re-rank's vector rows)
-        bytes_launch = float(row_b * stn[:, 0].sum() + 4 * gs * stn[:, 1].sum()
-                             + (128 * Ls * N_QUERIES if rr else 0))
-        achieved = bytes_launch / (ms / 1e3) / 1e9
-        out[name] = {"Ls": Ls, "rerank": Ls if rr else None, "qps": N_QUERIES / (ms / 1e3),
-                     "ms_per_step": ms, "recall_at_10": dict((a, b) for a, b in sweep)[Ls],
-                     "sweep_recall": sweep, "comps_per_query": float(stn[:, 0].mean()),
-                     "expansions_per_query": float(stn[:, 1].mean()),
-                     "algorithmic_gb_per_s": achieved, "frac_of_hbm_peak": achieved / peak}
+        # without an L2 window, then with one over this format's rows and over the graph
+        # (the window's persisting lines survive the flush: that is what it is for)
+        for window in (None, "codes" if rr else "rows", "graph"):
+            wb, hr = index.set_l2_window(window)
+            t = _timed_events(torch, stream, lambda: s.lanzar(q, ids, d, st, stream.cuda_stream),
+                              args.steps, args.warmup, flush)
+            stn = st.cpu().numpy().astype(np.int64)
+            ms = sum(t) / len(t)
+            row_b = 64 if rr else 128
+            # gathered rows + adjacency rows (+ the re-rank's vector rows)
+            bytes_launch = float(row_b * stn[:, 0].sum() + 4 * gs * stn[:, 1].sum()
+                                 + (128 * Ls * N_QUERIES if rr else 0))
+            achieved = bytes_launch / (ms / 1e3) / 1e9
+            key = name if window is None else f"{name}_l2_window_{window}"
+            out[key] = {"Ls": Ls, "rerank": Ls if rr else None, "qps": N_QUERIES / (ms / 1e3),
+                        "ms_per_step": ms, "recall_at_10": dict((a, b) for a, b in sweep)[Ls],
+                        "comps_per_query": float(stn[:, 0].mean()),
+                        "expansions_per_query": float(stn[:, 1].mean()),
+                        "algorithmic_gb_per_s": achieved, "frac_of_hbm_peak": achieved / peak}
+            if window is None:
+                out[key]["sweep_recall"] = sweep
+            else:
+                out[key]["l2_window"] = {"region": window, "bytes": wb, "hit_ratio": hr}
+        index.set_l2_window(None)
         s.liberar()
     c, v = out["code_rows"], out["vector_rows"]
     print(json.dumps({
@@ -750,6 +760,7 @@ def run_codes(args, local):
                    "code_step": step, "compress_s": compress_s,
                    "l2": "flushed (512 MiB write) before every timed step",
                    "code_rows": c, "vector_rows": v,
+                   "with_l2_window": {key: val for key, val in out.items() if "l2_window" in key},
                    "codes_over_vectors": c["qps"] / v["qps"]},
         "roofline": {"bound": "hbm", "achieved": c["algorithmic_gb_per_s"], "peak": peak,
                      "unit": "GB/s", "frac": c["frac_of_hbm_peak"], "traffic": None,

@@ -135,6 +135,24 @@ pgb_status pgb_index_get_info(const pgb_index* index, pgb_index_info* out);
 pgb_status pgb_file_check(const char* path, int kind, uint64_t info[4]);
 pgb_status pgb_index_destroy(pgb_index* index);
 
+/* L2 residency (no counterpart in the reference): an access-policy window over one region
+ * of a flat index -- PGB_L2_ROWS (the 128-byte vector rows), PGB_L2_CODES (the 64-byte
+ * code rows of pgb_index_compress) or PGB_L2_GRAPH (the adjacency rows) -- carried by every
+ * later flat search launch over the index (plain, compressed, batched, served, and CUDA
+ * graphs captured after the call). The window covers the region's first
+ * min(size, max_bytes (0: no limit), device maximum) bytes; the persisting set-aside of
+ * this process is set to min(window, device maximum), and window_bytes / hit_ratio (may
+ * be NULL) receive what was set. Lines in the window stay in L2 across launches and
+ * against other traffic. PGB_L2_NONE removes the window, demotes persisting lines and
+ * returns the set-aside to none (so does pgb_index_destroy). The set-aside is one per
+ * process: the last call made wins. */
+#define PGB_L2_NONE 0u
+#define PGB_L2_ROWS 1u
+#define PGB_L2_CODES 2u
+#define PGB_L2_GRAPH 3u
+pgb_status pgb_index_set_l2_window(pgb_index* index, uint32_t region, uint64_t max_bytes,
+                                   uint64_t* window_bytes, float* hit_ratio);
+
 /* ---- plain warp-per-query search (the drop-in) ------------------------------------ */
 /* preparar: scratch for up to max_queries queries with these params. */
 pgb_status pgb_searcher_create(pgb_index* index, uint32_t max_queries,

@@ -142,7 +142,7 @@ pgb_status enqueue(pgb_batch* b, const FlatPlan& P, const void* queries, uint32_
     A.gfilter = P.gfilter_words ? b->gfilter : nullptr;
     A.gvisited = P.gvisited_words ? b->gvisited : nullptr;
     A.queue = b->d_queue;
-    return launch_flat(P, A, st);
+    return launch_flat(P, A, st, ix);
 }
 
 pgb_status check_call(pgb_batch* b, const void* queries, uint32_t qstride, uint32_t* ids,

@@ -403,7 +403,59 @@ pgb_status pgb_index_get_info(const pgb_index* ix, pgb_index_info* out) {
     return PGB_OK;
 }
 
+pgb_status pgb_index_set_l2_window(pgb_index* ix, uint32_t region, uint64_t max_bytes,
+                                   uint64_t* window_bytes, float* hit_ratio) {
+    if (!ix) return fail(PGB_ERR_BAD_ARG, "null index");
+    if (ix->is_hnsw) return fail(PGB_ERR_BAD_ARG, "the L2 window applies to flat-graph searches");
+    const uint8_t* base = nullptr;
+    size_t size = 0;
+    switch (region) {
+        case PGB_L2_NONE: break;
+        case PGB_L2_ROWS: base = ix->rows; size = (size_t)kRowBytes * ix->n; break;
+        case PGB_L2_CODES:
+            if (!ix->codes) return fail(PGB_ERR_BAD_ARG, "index has no code rows (pgb_index_compress)");
+            base = ix->codes;
+            size = (size_t)kCodeRowBytes * ix->n;
+            break;
+        case PGB_L2_GRAPH: base = reinterpret_cast<const uint8_t*>(ix->adj); size = 4ull * ix->gs * ix->n; break;
+        default: return fail(PGB_ERR_BAD_ARG, "unknown L2 window region");
+    }
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e;
+    if (region == PGB_L2_NONE) {
+        // this process's set-aside back to none; persisting lines become normal lines
+        ix->l2_base = nullptr;
+        ix->l2_bytes = 0;
+        ix->l2_hit = 0.f;
+        e = cudaCtxResetPersistingL2Cache();
+        if (e == cudaSuccess) e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+        if (e != cudaSuccess) return cuda_fail(e, "L2 set-aside");
+        if (window_bytes) *window_bytes = 0;
+        if (hit_ratio) *hit_ratio = 0.f;
+        return PGB_OK;
+    }
+    int max_win = 0, max_persist = 0;
+    if ((e = cudaDeviceGetAttribute(&max_win, cudaDevAttrMaxAccessPolicyWindowSize, ix->device)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ix->device)) != cudaSuccess)
+        return cuda_fail(e, "L2 attributes");
+    if (max_win <= 0 || max_persist <= 0) return fail(PGB_ERR_BAD_ARG, "device has no persisting L2 lines");
+    size_t win = std::min(size, (size_t)max_win);
+    if (max_bytes) win = std::min(win, (size_t)max_bytes);
+    const size_t set_aside = std::min(win, (size_t)max_persist);
+    // the set-aside belongs to this process's context and ends with it
+    if ((e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, set_aside)) != cudaSuccess)
+        return cuda_fail(e, "L2 set-aside");
+    ix->l2_base = const_cast<uint8_t*>(base);
+    ix->l2_bytes = win;
+    ix->l2_hit = win ? std::min(1.f, (float)((double)set_aside / (double)win)) : 0.f;
+    if (window_bytes) *window_bytes = win;
+    if (hit_ratio) *hit_ratio = ix->l2_hit;
+    return PGB_OK;
+}
+
 pgb_status pgb_index_destroy(pgb_index* ix) {
+    if (ix && ix->l2_bytes) pgb_index_set_l2_window(ix, PGB_L2_NONE, 0, nullptr, nullptr);
     free_index(ix);
     return PGB_OK;
 }

@@ -47,6 +47,11 @@ struct pgb_index {
     uint8_t* code_off = nullptr;
     int32_t code_step = 0;
     int32_t code_off_host[PGB_MAX_DIM] = {0};
+    // L2 access-policy window given to every flat search launch over this index
+    // (pgb_index_set_l2_window): [l2_base, l2_base + l2_bytes) persists with ratio l2_hit
+    void* l2_base = nullptr;
+    size_t l2_bytes = 0;
+    float l2_hit = 0.f;
 };
 
 namespace pgb {

@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "errors.h"
+#include "index.h"
 #include "search_flat.cuh"
 #include "search_hnsw.h"
 #include "search_plan.h"
@@ -113,7 +114,7 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     return PGB_OK;
 }
 
-pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
+pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream, const pgb_index* ix) {
     A.L = P.L;
     A.gfilter_words = P.gfilter_words;
     A.gvisited_words = P.gvisited_words;
@@ -123,8 +124,27 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream) {
     if (P.batched)
         blocks = std::max(1, std::min(blocks, (int)((A.nq + P.warps_per_block - 1) / P.warps_per_block)));
     void* kern = (P.batched && !A.ls_arr) ? P.kernel_uniform : P.kernel;
-    cudaError_t e = cudaLaunchKernel(kern, dim3(blocks), dim3(P.warps_per_block * 32), args,
-                                     P.smem_bytes, stream);
+    cudaError_t e;
+    if (ix && ix->l2_bytes) {
+        // the index's persisting window travels with the launch (and into a captured graph)
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(blocks);
+        cfg.blockDim = dim3(P.warps_per_block * 32);
+        cfg.dynamicSmemBytes = P.smem_bytes;
+        cfg.stream = stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        at[0].val.accessPolicyWindow.base_ptr = ix->l2_base;
+        at[0].val.accessPolicyWindow.num_bytes = ix->l2_bytes;
+        at[0].val.accessPolicyWindow.hitRatio = ix->l2_hit;
+        at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelExC(&cfg, kern, args);
+    } else {
+        e = cudaLaunchKernel(kern, dim3(blocks), dim3(P.warps_per_block * 32), args, P.smem_bytes, stream);
+    }
     if (e != cudaSuccess)
         return fail(PGB_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
     return PGB_OK;

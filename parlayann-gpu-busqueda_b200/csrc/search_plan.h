@@ -45,6 +45,8 @@ int flat_chunks_for(uint32_t deg_lim);
 pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P);
 // A's table pointers must cover P.total_warps slices when the plan keeps them global.
 // A batched launch with A.ls_arr == nullptr runs the uniform kernel on (A.Ls, A.k).
-pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream);
+// ix (optional): the index whose L2 access-policy window, when set, the launch carries.
+pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream,
+                       const pgb_index* ix = nullptr);
 
 }  // namespace pgb

@@ -170,7 +170,7 @@ pgb_status pgb_searcher_search(pgb_searcher* S, const void* queries, uint32_t nq
     A.stats = stats;
     A.gfilter = S->gfilter;
     A.gvisited = S->gvisited;
-    if (!S->codes) return launch_flat(S->flat, A, st);
+    if (!S->codes) return launch_flat(S->flat, A, st, ix);
     // code rows: the search keeps the first `rerank` entries of each frontier, then the
     // exact re-rank writes the caller's k
     A.rows = ix->codes;
@@ -180,7 +180,7 @@ pgb_status pgb_searcher_search(pgb_searcher* S, const void* queries, uint32_t nq
     A.out_stride = S->rerank;
     A.ids = S->cand;
     A.dists = S->cand_d;
-    pgb_status s = launch_flat(S->flat, A, st);
+    pgb_status s = launch_flat(S->flat, A, st, ix);
     if (s != PGB_OK) return s;
     return rerank_launch(ix, queries, nq, query_stride, S->cand, S->rerank, p.k, ids, dists, st);
 }

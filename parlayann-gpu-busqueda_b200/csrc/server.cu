@@ -266,7 +266,7 @@ bool launch(pgb_server* S, Context& c) {
     A.gfilter = c.gfilter;
     A.gvisited = c.gvisited;
     A.queue = c.d_queue;
-    if (launch_flat(S->plan, A, c.stream) != PGB_OK) {
+    if (launch_flat(S->plan, A, c.stream, ix) != PGB_OK) {
         fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
         return false;
     }

@@ -108,6 +108,16 @@ class Index:
         self.info = N.IndexInfo()
         N.check(N.lib.pgb_index_get_info(self._h, C.byref(self.info)))
 
+    def set_l2_window(self, region: str, max_bytes: int = 0):
+        """Persisting L2 window over "rows", "codes" or "graph" (None / "none" removes it),
+        carried by every later flat search launch; returns (window bytes, hit ratio)."""
+        r = {None: N.L2_NONE, "none": N.L2_NONE, "rows": N.L2_ROWS, "codes": N.L2_CODES,
+             "graph": N.L2_GRAPH}[region]
+        wb, hr = C.c_uint64(), C.c_float()
+        N.check(N.lib.pgb_index_set_l2_window(self._h, r, int(max_bytes), C.byref(wb),
+                                              C.byref(hr)))
+        return wb.value, hr.value
+
     def codes(self, rows: bool = True):
         """(step, offsets int32 [dim], code rows uint8 [n, 64] or None)."""
         step = C.c_int32()
