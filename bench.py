@@ -322,7 +322,8 @@ def run_profile_hnsw(args, local):
 
 
 def run_profile(args, local):
-    """Launches only the search kernels (plain, then batched) on a small query set."""
+    """Launches only the search kernels (plain, then batched) on a small query set; with
+    --workload codes the plain launches search the 4-bit code rows (+ the re-rank)."""
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -330,9 +331,12 @@ def run_profile(args, local):
     base, queries, graph = load_workload(pgb, 0, lambda: None)
     nq, Ls = args.profile_nq, args.profile_ls
     index = pgb.Index.flat(base, graph, device=local)
+    codes = args.workload == "codes"
+    if codes:
+        index.compress()
     q = torch.from_numpy(np.ascontiguousarray(queries[:nq]).view(np.uint8)).to(dev)
     sp = torch.cuda.current_stream(dev).cuda_stream
-    s = pgb.Searcher(index, nq, pgb.QueryParams(k=K, beam_size=Ls))
+    s = pgb.Searcher(index, nq, pgb.QueryParams(k=K, beam_size=Ls), rerank=Ls if codes else 0)
     ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
     d = torch.empty_like(ids)
     st = torch.empty((nq, 4), dtype=torch.int32, device=dev)
