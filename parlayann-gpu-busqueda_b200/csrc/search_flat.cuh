@@ -327,17 +327,13 @@ __device__ __forceinline__ void sort_keys(uint64_t* keys, int nc, int lane) {
 #ifndef PGB_DIST_SLOTS
 #define PGB_DIST_SLOTS 2
 #endif
-template <bool Signed, int SLOTS = PGB_DIST_SLOTS>
-__device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
-                                              const uint32_t* ids, int32_t* out, int np,
-                                              const int4* q4, const int32_t qq, uint32_t dim,
-                                              bool norm_in_row, int lane) {
-    const int grp = lane >> 2, c = lane & 3;
-    const int4 qa = q4[c], qb = q4[c + 4];
-    // bytes past dim are zero in every row; lane 3 also loads word 7 when it holds the norm
-    const bool need_a = (uint32_t)(c * 16) < dim;
-    const bool need_b = (uint32_t)((c + 4) * 16) < dim || (norm_in_row && c == 3);
-    for (int base = 0; base < np; base += 8 * SLOTS) {
+// one round: rows base .. base + 8*SLOTS - 1 (those past np are not stored)
+template <bool Signed, int SLOTS>
+__device__ __forceinline__ void row_round(const uint8_t* __restrict__ rows, const uint32_t* ids,
+                                          int32_t* out, int np, int base, const int4 qa,
+                                          const int4 qb, const int32_t qq, bool need_a,
+                                          bool need_b, bool norm_in_row, int grp, int c) {
+    {
         int4 va[SLOTS], vb[SLOTS];
 #pragma unroll
         for (int r = 0; r < SLOTS; r++) {
@@ -370,6 +366,28 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
                 if (i < np) out[i] = qq + t[r];
             }
         }
+    }
+}
+
+// TAIL: a tail of at most 8 rows takes a one-slot round (fewer instructions per
+// expansion; the batched kernels use it: +1 % there, while the plain kernel's register
+// budget spills more with it and loses 3 %)
+template <bool Signed, int SLOTS = PGB_DIST_SLOTS, bool TAIL = false>
+__device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
+                                              const uint32_t* ids, int32_t* out, int np,
+                                              const int4* q4, const int32_t qq, uint32_t dim,
+                                              bool norm_in_row, int lane) {
+    const int grp = lane >> 2, c = lane & 3;
+    const int4 qa = q4[c], qb = q4[c + 4];
+    // bytes past dim are zero in every row; lane 3 also loads word 7 when it holds the norm
+    const bool need_a = (uint32_t)(c * 16) < dim;
+    const bool need_b = (uint32_t)((c + 4) * 16) < dim || (norm_in_row && c == 3);
+    for (int base = 0; base < np; base += 8 * SLOTS) {
+        if (TAIL && SLOTS > 1 && np - base <= 8) {
+            row_round<Signed, 1>(rows, ids, out, np, base, qa, qb, qq, need_a, need_b, norm_in_row, grp, c);
+            break;
+        }
+        row_round<Signed, SLOTS>(rows, ids, out, np, base, qa, qb, qq, need_a, need_b, norm_in_row, grp, c);
     }
     __syncwarp();
 }
@@ -441,17 +459,18 @@ __device__ __forceinline__ int32_t query_sq_norm(const int4* q4, int lane) {
 // computes with the same make_flat_layout.
 // C4: A.rows holds 4-bit code rows (kCodeRowBytes each) and distances are those of the
 // reconstructed vectors (code_row_distances); otherwise 128-byte vector rows.
-template <bool Signed, bool C4>
+// TAIL: row_distances' one-slot tail round (the batched kernels).
+template <bool Signed, bool C4, bool TAIL>
 __device__ __forceinline__ void pending_distances(const FlatArgs& A, const uint32_t* ids,
                                                   int32_t* out, int np, const int4* q4,
                                                   int32_t qq, bool nir, int lane) {
     if constexpr (C4)
         code_row_distances<Signed>(A.rows, ids, out, np, q4, qq, A.code_step, lane);
     else
-        row_distances<Signed>(A.rows, ids, out, np, q4, qq, A.dim, nir, lane);
+        row_distances<Signed, PGB_DIST_SLOTS, TAIL>(A.rows, ids, out, np, q4, qq, A.dim, nir, lane);
 }
 
-template <int CH, bool Signed, int FW, bool C4 = false>
+template <int CH, bool Signed, int FW, bool C4 = false, bool TAIL = false>
 __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfilter,
                            uint32_t* gvisited, uint32_t q, uint32_t Ls, uint32_t k, int lane) {
     constexpr bool SFILT = FW > 0;
@@ -503,7 +522,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
     if (lane == 0) pend[0] = A.start;
     __syncwarp();
     const bool nir = A.norm_in_row != 0;
-    pending_distances<Signed, C4>(A, pend, pdist, 1, q4, qq, nir, lane);
+    pending_distances<Signed, C4, TAIL>(A, pend, pdist, 1, q4, qq, nir, lane);
     if (lane == 0) {
         fkey[0] = pack_key(pdist[0], A.start);
         fvis[0] = 0;
@@ -633,7 +652,7 @@ __device__ void flat_query(const FlatArgs& A, unsigned char* wmem, uint32_t* gfi
         PGB_PROF_ADD(SEC_FILTER, tp);
 
         // ---- distances ------------------------------------------------------------
-        pending_distances<Signed, C4>(A, pend, pdist, np, q4, qq, nir, lane);
+        pending_distances<Signed, C4, TAIL>(A, pend, pdist, np, q4, qq, nir, lane);
         PGB_PROF_ADD(SEC_DIST, tp);
 
         // ---- candidates under the cutoff, in arrival order ------------------------

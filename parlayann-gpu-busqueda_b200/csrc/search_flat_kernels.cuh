@@ -81,9 +81,9 @@ __global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_batched_kernel(FlatA
         if (slot >= A.nq) break;
         const uint32_t q = A.order[slot];
         if (UNI)
-            flat_query<CH, Signed, FW>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
+            flat_query<CH, Signed, FW, false, true>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
         else
-            flat_query<CH, Signed, FW>(A, wmem, gf, gv, q, A.ls_arr[q], A.k_arr[q], lane);
+            flat_query<CH, Signed, FW, false, true>(A, wmem, gf, gv, q, A.ls_arr[q], A.k_arr[q], lane);
     }
     PGB_PROF_EXIT();
 }
