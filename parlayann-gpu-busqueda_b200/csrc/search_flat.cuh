@@ -398,6 +398,36 @@ __device__ __forceinline__ void row_distances(const uint8_t* __restrict__ rows,
 //   ||q - v||^2 = (||q||^2 - 2 q.offset) - 2 step (q.code) + ||v||^2,
 // where qq carries the first term and ||v||^2 sits in bytes 60..63 (word 3's last int,
 // held by lane 3; the query is zero over those dimensions, so its codes add nothing).
+// One round: code rows base .. base + 8*SLOTS - 1 (those past np are not stored).
+template <bool Signed, int SLOTS>
+__device__ __forceinline__ void code_round(const uint8_t* __restrict__ codes, const uint32_t* ids,
+                                           int32_t* out, int np, int base, const int4 qa,
+                                           const int4 qb, const int32_t qq, int32_t step,
+                                           int grp, int c) {
+    int4 v[SLOTS];
+#pragma unroll
+    for (int r = 0; r < SLOTS; r++) {
+        const int i = base + r * 8 + grp;
+        // slots past np re-read row ids[0], as in row_distances
+        v[r] = ldg16(codes + (size_t)ids[i < np ? i : 0] * kCodeRowBytes + c * 16);
+    }
+    int32_t t[SLOTS];
+#pragma unroll
+    for (int r = 0; r < SLOTS; r++)
+        t[r] = (c == 3 ? v[r].w : 0) - 2 * step * code_dot<Signed>(v[r], qa, qb);
+#pragma unroll
+    for (int off = 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int r = 0; r < SLOTS; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 4);
+    if (c == 0) {
+#pragma unroll
+        for (int r = 0; r < SLOTS; r++) {
+            const int i = base + r * 8 + grp;
+            if (i < np) out[i] = qq + t[r];
+        }
+    }
+}
+
 template <bool Signed, int SLOTS = PGB_DIST_SLOTS>
 __device__ __forceinline__ void code_row_distances(const uint8_t* __restrict__ codes,
                                                    const uint32_t* ids, int32_t* out, int np,
@@ -406,28 +436,13 @@ __device__ __forceinline__ void code_row_distances(const uint8_t* __restrict__ c
     const int grp = lane >> 2, c = lane & 3;
     const int4 qa = q4[2 * c], qb = q4[2 * c + 1];
     for (int base = 0; base < np; base += 8 * SLOTS) {
-        int4 v[SLOTS];
-#pragma unroll
-        for (int r = 0; r < SLOTS; r++) {
-            const int i = base + r * 8 + grp;
-            // slots past np re-read row ids[0], as in row_distances
-            v[r] = ldg16(codes + (size_t)ids[i < np ? i : 0] * kCodeRowBytes + c * 16);
+        // a tail of at most 8 rows takes a one-slot round (the code-row kernel has the
+        // registers for both loop bodies)
+        if (SLOTS > 1 && np - base <= 8) {
+            code_round<Signed, 1>(codes, ids, out, np, base, qa, qb, qq, step, grp, c);
+            break;
         }
-        int32_t t[SLOTS];
-#pragma unroll
-        for (int r = 0; r < SLOTS; r++)
-            t[r] = (c == 3 ? v[r].w : 0) - 2 * step * code_dot<Signed>(v[r], qa, qb);
-#pragma unroll
-        for (int off = 2; off > 0; off >>= 1)
-#pragma unroll
-            for (int r = 0; r < SLOTS; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, 4);
-        if (c == 0) {
-#pragma unroll
-            for (int r = 0; r < SLOTS; r++) {
-                const int i = base + r * 8 + grp;
-                if (i < np) out[i] = qq + t[r];
-            }
-        }
+        code_round<Signed, SLOTS>(codes, ids, out, np, base, qa, qb, qq, step, grp, c);
     }
     __syncwarp();
 }
