@@ -6,15 +6,15 @@
  *
  * What each group replaces in the reference (paths inside the reference project):
  *   pgb_index_*     <- subirVectores / subirGrafo / subirHnsw + the readers
- *                      (cuda/datos_gpu.cu:61-122, cuda/busqueda_hnsw.cu:462-530,
- *                      cuda/lectores.cpp:113-187, cuda/hnsw_lector.cpp:336-419)
+ *                      (cuda/datos_gpu.cu:8-81, cuda/busqueda_hnsw.cu:462-530,
+ *                      cuda/lectores.cpp:62-170, cuda/hnsw_lector.cpp:14-111)
  *   pgb_searcher_*  <- BuscadorGPU / BuscadorHnsw preparar, lanzar, liberar
  *                      (cuda/busqueda.cuh:36-61, cuda/busqueda.cu:525-594,
  *                      cuda/hnsw.h:65-86, cuda/busqueda_hnsw.cu:551-645)
  *   pgb_query_params <- ConfigBusqueda (cuda/busqueda.cuh:6-11) extended to ParlayANN's
  *                      QueryParams{k, beamSize, cut, limit, degree_limit}
  *   pgb_query_stats <- compDev / banderasDev (cuda/busqueda.cuh:43-46) + expansions
- *   pgb_recall      <- calcularRecall (cuda/evaluacion.cpp:184-208)
+ *   pgb_recall      <- calcularRecall (cuda/evaluacion.cpp:56-80)
  *   pgb_batch_*, pgb_server_* have no counterpart in the reference: the batched
  *                      persistent form and the serving loop built on top of the plain
  *                      warp-per-query search, returning identical neighbours.
@@ -130,10 +130,21 @@ pgb_status pgb_index_load_hnsw(int device, const char* vectors_path, pgb_elem el
 pgb_status pgb_index_get_info(const pgb_index* index, pgb_index_info* out);
 /* Reads and checks a file on the host only (no GPU): kind 0 = vectors, 1 = flat graph,
  * 2 = HNSW v3 model, with the reference readers' checks (exact size / end of file, ids in
- * range; cuda/lectores.cpp:113-187, cuda/hnsw_lector.cpp:336-419). info (may be NULL)
+ * range; cuda/lectores.cpp:62-170, cuda/hnsw_lector.cpp:14-111). info (may be NULL)
  * receives {n, dim | max degree | dim, total bytes | edges | lists, 0 | 0 | entries}. */
 pgb_status pgb_file_check(const char* path, int kind, uint64_t info[4]);
 pgb_status pgb_index_destroy(pgb_index* index);
+
+/* Exact squared L2 distances of (query, point) pairs, computed by the search kernels' own
+ * row code (dp4a over 128-byte rows): the library's form of the reference's load-and-verify
+ * step (cuda/paso1_carga.cu:33-123), which checks GPU distances of random and ground-truth
+ * pairs against the CPU distance (cuda/lectores.cpp:172-179). Device pointers: queries (nq
+ * rows of index dim bytes, query_stride apart), pairs[2 * npairs] = (query row, point id)
+ * and out[npairs] (int32). Synchronous on `stream`. A pair naming a query >= nq or a point
+ * >= n gets INT32_MIN and the call returns PGB_ERR_BAD_ARG. */
+pgb_status pgb_index_distances(const pgb_index* index, const void* queries, uint32_t nq,
+                               uint32_t query_stride, const uint32_t* pairs, uint64_t npairs,
+                               int32_t* out, void* stream);
 
 /* L2 residency (no counterpart in the reference): an access-policy window over one region
  * of a flat index -- PGB_L2_ROWS (the 128-byte vector rows), PGB_L2_CODES (the 64-byte
@@ -241,12 +252,15 @@ typedef struct pgb_batch_options {
     uint32_t warps_per_block;   /* 1, 2 or 4; 0: default (4) / tuned                    */
     uint32_t filter_placement;  /* 0 auto, 1 shared memory (max_beam <= 128), 2 global  */
     uint32_t visited_placement; /* 0 auto, 1 shared memory, 2 global memory             */
+    uint32_t queries_per_warp;  /* 1: one query per warp; 2: one per 16-lane half (rows
+                                   of up to 128 neighbours); 0: 1 untuned / tuned        */
 } pgb_batch_options;
 
 typedef struct pgb_batch_config {
     uint32_t warps_per_block, blocks, filter_in_shared, visited_in_shared;
     uint32_t shared_bytes_per_warp;
     float tuned_ms;             /* time of the chosen config in the last tune (0: untuned) */
+    uint32_t queries_per_warp;  /* 1 or 2 (paired 16-lane halves)                          */
 } pgb_batch_config;
 
 pgb_status pgb_batch_create(pgb_index* index, const pgb_batch_options* opt, pgb_batch** out);

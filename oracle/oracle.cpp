@@ -11,8 +11,8 @@
 //   * exact visited multiset: cuda/busqueda.cu:57-82, overflow rule :205-208
 //   * HNSW layered search   : cuda/busqueda_hnsw.cu:215-456 (kernelHnsw)
 //   * filter sizes          : cuda/busqueda.cu:536-540, cuda/busqueda_hnsw.cu:556-559
-//   * distance              : cuda/lectores.cpp:215-222 (distanciaCPU)
-//   * recall with ties      : cuda/evaluacion.cpp:184-208 (calcularRecall)
+//   * distance              : cuda/lectores.cpp:172-179 (distanciaCPU)
+//   * recall with ties      : cuda/evaluacion.cpp:56-80 (calcularRecall)
 // The flat search is written the way ParlayANN writes beam_search (std::set_union /
 // std::set_difference on (dist, id)-sorted vectors) so that the multiset semantics the
 // reference emulates with copy counts come out of the STL algorithms themselves.
@@ -87,7 +87,7 @@ struct Vectors {
     const uint8_t* row(uint32_t i) const { return data + (size_t)i * stride; }
 };
 
-// squared L2 in exact integer arithmetic (cuda/lectores.cpp:215-222)
+// squared L2 in exact integer arithmetic (cuda/lectores.cpp:172-179)
 inline int32_t sq_l2(const uint8_t* a, const uint8_t* b, uint32_t dim, int is_signed) {
     int32_t s = 0;
     if (is_signed) {
@@ -396,7 +396,7 @@ int oracle_hnsw_search(const uint8_t* base, uint32_t dim, uint32_t base_stride, 
     return 0;
 }
 
-// recall@k with distance ties (cuda/evaluacion.cpp:184-208)
+// recall@k with distance ties (cuda/evaluacion.cpp:56-80)
 double oracle_recall(const uint32_t* gt_ids, const float* gt_dists, uint32_t nq, uint32_t gt_k,
                      const uint32_t* ids, uint32_t k) {
     long long total = 0;

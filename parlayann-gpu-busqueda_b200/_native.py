@@ -82,6 +82,7 @@ _sig("pgb_searcher_search", C.c_int, vp, vp, u32, u32, vp, vp, vp, vp)
 _sig("pgb_searcher_search_host", C.c_int, vp, vp, u32, u32, vp, vp, vp)
 _sig("pgb_searcher_destroy", C.c_int, vp)
 _sig("pgb_index_compress", C.c_int, vp, i32, vp)
+_sig("pgb_index_distances", C.c_int, vp, vp, u32, u32, vp, u64, vp, vp)
 _sig("pgb_index_set_l2_window", C.c_int, vp, u32, u64, C.POINTER(u64), C.POINTER(C.c_float))
 L2_NONE, L2_ROWS, L2_CODES, L2_GRAPH = 0, 1, 2, 3
 _sig("pgb_index_get_codes", C.c_int, vp, C.POINTER(i32), vp, vp)
@@ -123,13 +124,14 @@ class BatchOptions(C.Structure):
                 ("cut", C.c_double), ("limit", C.c_int64), ("degree_limit", C.c_uint32),
                 ("exclude_query_id", C.c_uint32), ("query_id_base", C.c_uint32),
                 ("warps_per_block", C.c_uint32), ("filter_placement", C.c_uint32),
-                ("visited_placement", C.c_uint32)]
+                ("visited_placement", C.c_uint32), ("queries_per_warp", C.c_uint32)]
 
 
 class BatchConfig(C.Structure):
     _fields_ = [("warps_per_block", C.c_uint32), ("blocks", C.c_uint32),
                 ("filter_in_shared", C.c_uint32), ("visited_in_shared", C.c_uint32),
-                ("shared_bytes_per_warp", C.c_uint32), ("tuned_ms", C.c_float)]
+                ("shared_bytes_per_warp", C.c_uint32), ("tuned_ms", C.c_float),
+                ("queries_per_warp", C.c_uint32)]
 
 
 _sig("pgb_batch_create", C.c_int, vp, C.POINTER(BatchOptions), C.POINTER(vp))

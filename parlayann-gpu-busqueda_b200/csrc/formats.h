@@ -7,7 +7,7 @@
 //                                                          (cuda/hnsw.h:11-16)
 //   GT      : [nq u32][k u32][ids nq*k u32][dists nq*k f32] (cuda/lectores.h:29-36)
 // Every reader checks the exact file size / end of file and the id ranges, as the
-// reference readers do (cuda/lectores.cpp:123-185, cuda/hnsw_lector.cpp:392-417), but
+// reference readers do (cuda/lectores.cpp:62-144, cuda/hnsw_lector.cpp:14-111), but
 // reports a status instead of exiting.
 #pragma once
 

@@ -1,7 +1,7 @@
 // index.cu -- index creation: uploads and device-side re-layout of vectors and graphs.
-// Replaces subirVectores / subirGrafo / subirHnsw (reference cuda/datos_gpu.cu:61-122,
+// Replaces subirVectores / subirGrafo / subirHnsw (reference cuda/datos_gpu.cu:8-81,
 // cuda/busqueda_hnsw.cu:462-530). Padding happens on the device, so no padded host
-// copy (the reference builds up to 600 MB on the host, cuda/datos_gpu.cu:109-111).
+// copy (the reference builds up to 600 MB on the host, cuda/datos_gpu.cu:68-72).
 #include <algorithm>
 #include <cstring>
 #include <string>

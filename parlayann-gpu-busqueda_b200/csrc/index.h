@@ -8,7 +8,7 @@
 //                padded with 0xFFFFFFFF (reference GrafoGPU, cuda/datos_gpu.h:19-28)
 //   HNSW       : level-0 matrix n x g0s; upper levels one block of gas ids per
 //                (node, level >= 1) at upper_start[node] + level - 1; vectors in node
-//                order (reference HnswGPU, cuda/hnsw.h:60-80)
+//                order (reference HnswGPU, cuda/hnsw.h:37-59)
 #pragma once
 
 #include <cuda_runtime.h>

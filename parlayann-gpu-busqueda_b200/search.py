@@ -52,9 +52,10 @@ class QueryParams:
 class Index:
     """Device-resident index (vectors + graph). Read-only after creation."""
 
-    def __init__(self, handle: int, dtype):
+    def __init__(self, handle: int, dtype, device: int = 0):
         self._h = C.c_void_p(handle)
         self.dtype = np.dtype(dtype)
+        self.device = device
         info = N.IndexInfo()
         N.check(N.lib.pgb_index_get_info(self._h, C.byref(info)))
         self.info = info
@@ -68,7 +69,7 @@ class Index:
         N.check(N.lib.pgb_index_create_flat(device, _ptr(v), v.shape[0], v.shape[1],
                                             _elem(v.dtype), _ptr(deg),
                                             _ptr(edges) if edges.size else 0, C.byref(h)))
-        return cls(h.value, v.dtype)
+        return cls(h.value, v.dtype, device)
 
     @classmethod
     def hnsw(cls, vectors: np.ndarray, h: Hnsw, device: int = 0) -> "Index":
@@ -79,21 +80,21 @@ class Index:
         N.check(N.lib.pgb_index_create_hnsw(device, _ptr(v), v.shape[0], v.shape[1],
                                             _elem(v.dtype), h.n, *[_ptr(a) for a in arrs[:4]],
                                             _ptr(arrs[4]), len(arrs[4]), C.byref(out)))
-        return cls(out.value, v.dtype)
+        return cls(out.value, v.dtype, device)
 
     @classmethod
     def load_flat(cls, vectors_path: str, graph_path: str, dtype=np.int8, device: int = 0):
         h = C.c_void_p()
         N.check(N.lib.pgb_index_load_flat(device, vectors_path.encode(), _elem(dtype),
                                           graph_path.encode(), C.byref(h)))
-        return cls(h.value, dtype)
+        return cls(h.value, dtype, device)
 
     @classmethod
     def load_hnsw(cls, vectors_path: str, hnsw_path: str, dtype=np.int8, device: int = 0):
         h = C.c_void_p()
         N.check(N.lib.pgb_index_load_hnsw(device, vectors_path.encode(), _elem(dtype),
                                           hnsw_path.encode(), C.byref(h)))
-        return cls(h.value, dtype)
+        return cls(h.value, dtype, device)
 
     @property
     def handle(self):
@@ -117,6 +118,21 @@ class Index:
         N.check(N.lib.pgb_index_set_l2_window(self._h, r, int(max_bytes), C.byref(wb),
                                               C.byref(hr)))
         return wb.value, hr.value
+
+    def distances(self, queries, pairs, stream: int = 0) -> np.ndarray:
+        """Exact int32 squared L2 of (query row, point id) pairs by the search kernels' row
+        code. queries: [nq, dim] (numpy or CUDA tensor); pairs: [npairs, 2] uint32."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        q = queries if hasattr(queries, "data_ptr") else torch.from_numpy(
+            np.ascontiguousarray(queries).view(np.uint8)).to(dev)
+        pr = pairs if hasattr(pairs, "data_ptr") else torch.from_numpy(
+            np.ascontiguousarray(pairs, dtype=np.uint32).view(np.int32)).to(dev)
+        npairs = pr.shape[0]
+        out = torch.empty(max(1, npairs), dtype=torch.int32, device=dev)
+        N.check(N.lib.pgb_index_distances(self._h, _ptr(q), q.shape[0], q.stride(0), _ptr(pr),
+                                          npairs, _ptr(out), C.c_void_p(stream)))
+        return out[:npairs].cpu().numpy()
 
     def codes(self, rows: bool = True):
         """(step, offsets int32 [dim], code rows uint8 [n, 64] or None)."""
@@ -202,7 +218,7 @@ class Searcher:
 
 def recall(gt_ids: np.ndarray, gt_dists: np.ndarray, ids: np.ndarray, k: int) -> float:
     """recall@k with distance ties (big-ann-benchmarks compute_recall_with_distance_ties;
-    reference cuda/evaluacion.cpp:184-208)."""
+    reference cuda/evaluacion.cpp:56-80)."""
     gi = np.ascontiguousarray(gt_ids, dtype=np.uint32)
     gd = np.ascontiguousarray(gt_dists, dtype=np.float32)
     ii = np.ascontiguousarray(ids[:, :k], dtype=np.uint32)
@@ -307,11 +323,13 @@ class Batch:
     def __init__(self, index: Index, max_queries: int, max_beam: int, max_k: int,
                  cut: float = 1.35, limit: int = 0, degree_limit: int = 0,
                  exclude_query_id: bool = True, query_id_base: int = 0,
-                 warps_per_block: int = 0, filter_placement: int = 0, visited_placement: int = 0):
+                 warps_per_block: int = 0, filter_placement: int = 0, visited_placement: int = 0,
+                 queries_per_warp: int = 0):
         self.index, self.max_k = index, max_k
         self._opt = N.BatchOptions(max_queries, max_beam, max_k, float(cut), int(limit),
                                    degree_limit, 1 if exclude_query_id else 0, query_id_base,
-                                   warps_per_block, filter_placement, visited_placement)
+                                   warps_per_block, filter_placement, visited_placement,
+                                   queries_per_warp)
         h = C.c_void_p()
         N.check(N.lib.pgb_batch_create(index.handle, C.byref(self._opt), C.byref(h)))
         self._h = h

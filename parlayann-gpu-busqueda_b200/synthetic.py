@@ -51,7 +51,7 @@ class MixtureLaw:
         return out
 
 
-# C1 small plain method; C2/C3/C5 1M int8; C4 10M uint8
+# mixture laws of the workloads: C1 10k int8 d=100 (64 centres); C2-C3-C5 1M int8 d=100 (1,024 centres); C4 10M uint8 d=128 (4,096 centres)
 LAW_C1 = MixtureLaw(dim=100, n_centers=64, center_lo=-40, center_hi=40, sigma=12,
                     zero_frac=0.0, signed=True)
 LAW_C2 = MixtureLaw(dim=100, n_centers=1024, center_lo=-40, center_hi=40, sigma=10,

@@ -1,7 +1,7 @@
 """File formats: Python writers/readers round-trip, and the C readers (the ones the index
 loaders use) accept good files and reject truncated or corrupt ones with a status, as the
-reference readers reject them with an exit (cuda/lectores.cpp:113-187,
-cuda/hnsw_lector.cpp:336-419)."""
+reference readers reject them with an exit (cuda/lectores.cpp:62-170,
+cuda/hnsw_lector.cpp:14-111)."""
 import os
 import struct
 

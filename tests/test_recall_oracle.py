@@ -3,7 +3,7 @@ import numpy as np
 
 
 def recall_py(gt_ids, gt_d, ids, k):
-    """Plain restatement of compute_recall_with_distance_ties (cuda/evaluacion.cpp:184-208)."""
+    """Plain restatement of compute_recall_with_distance_ties (cuda/evaluacion.cpp:56-80)."""
     total = 0
     for q in range(len(gt_ids)):
         end = gt_ids.shape[1]
