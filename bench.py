@@ -340,8 +340,8 @@ def run_profile(args, local):
     ids = torch.empty((nq, K), dtype=torch.int32, device=dev)
     d = torch.empty_like(ids)
     st = torch.empty((nq, 4), dtype=torch.int32, device=dev)
-    b = pgb.Batch(index, nq, max_beam=Ls, max_k=K, warps_per_block=4, filter_placement=1,
-                  visited_placement=2)
+    b = pgb.Batch(index, nq, max_beam=Ls, max_k=K, warps_per_block=args.profile_wpb,
+                  filter_placement=1, visited_placement=2)
     b.plan(np.full(nq, Ls, np.uint32), np.full(nq, K, np.uint32))
     for _ in range(args.warmup + args.steps):
         s.lanzar(q, ids, d, st, sp)
@@ -373,6 +373,8 @@ def main():
                          "warm-up then --steps launches of each kernel, nothing else")
     ap.add_argument("--profile-nq", type=int, default=8192)
     ap.add_argument("--profile-ls", type=int, default=40)
+    ap.add_argument("--profile-wpb", type=int, default=4,
+                    help="warps per block of the profiled batched launch")
     ap.add_argument("--workload", default="vamana",
                     choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "mixed_hnsw", "serving",
                              "serving_hnsw", "c4", "build", "codes"],

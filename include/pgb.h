@@ -252,15 +252,12 @@ typedef struct pgb_batch_options {
     uint32_t warps_per_block;   /* 1, 2 or 4; 0: default (4) / tuned                    */
     uint32_t filter_placement;  /* 0 auto, 1 shared memory (max_beam <= 128), 2 global  */
     uint32_t visited_placement; /* 0 auto, 1 shared memory, 2 global memory             */
-    uint32_t queries_per_warp;  /* 1: one query per warp; 2: one per 16-lane half (rows
-                                   of up to 128 neighbours); 0: 1 untuned / tuned        */
 } pgb_batch_options;
 
 typedef struct pgb_batch_config {
     uint32_t warps_per_block, blocks, filter_in_shared, visited_in_shared;
     uint32_t shared_bytes_per_warp;
     float tuned_ms;             /* time of the chosen config in the last tune (0: untuned) */
-    uint32_t queries_per_warp;  /* 1 or 2 (paired 16-lane halves)                          */
 } pgb_batch_config;
 
 pgb_status pgb_batch_create(pgb_index* index, const pgb_batch_options* opt, pgb_batch** out);

@@ -124,14 +124,13 @@ class BatchOptions(C.Structure):
                 ("cut", C.c_double), ("limit", C.c_int64), ("degree_limit", C.c_uint32),
                 ("exclude_query_id", C.c_uint32), ("query_id_base", C.c_uint32),
                 ("warps_per_block", C.c_uint32), ("filter_placement", C.c_uint32),
-                ("visited_placement", C.c_uint32), ("queries_per_warp", C.c_uint32)]
+                ("visited_placement", C.c_uint32)]
 
 
 class BatchConfig(C.Structure):
     _fields_ = [("warps_per_block", C.c_uint32), ("blocks", C.c_uint32),
                 ("filter_in_shared", C.c_uint32), ("visited_in_shared", C.c_uint32),
-                ("shared_bytes_per_warp", C.c_uint32), ("tuned_ms", C.c_float),
-                ("queries_per_warp", C.c_uint32)]
+                ("shared_bytes_per_warp", C.c_uint32), ("tuned_ms", C.c_float)]
 
 
 _sig("pgb_batch_create", C.c_int, vp, C.POINTER(BatchOptions), C.POINTER(vp))

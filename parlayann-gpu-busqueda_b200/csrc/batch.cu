@@ -3,10 +3,9 @@
 // plan   : host step, per-query (Ls, k) -> longest-beam-first work order on the device
 // search : cudaMemsetAsync(counter) + one persistent launch (capturable); a plan whose
 //          queries all share one (Ls, k) runs the uniform-batch kernel
-// tune   : times candidate (queries per warp, warps per block, filter / visited
-//          placement) on the planned queries and keeps the fastest; every candidate returns
-//          identical neighbours: one query per warp runs flat_query, two per warp run its
-//          16-lane restatement (flat_pair_run), the same integers in the same order
+// tune   : times candidate (warps per block, filter / visited placement) on the planned
+//          queries and keeps the fastest; every candidate returns identical neighbours,
+//          because all of them run the same per-query code (flat_query)
 // An HNSW index runs the HNSW kernel with each query at its own (Ls, k), its tables sized
 // for max_beam; it has a single launch shape, so tune only times it.
 #include <algorithm>
@@ -51,14 +50,13 @@ struct pgb_batch {
 namespace pgb {
 namespace {
 
-pgb_status make_plan(pgb_batch* b, int qpw, int wpb, int filter_pl, int visited_pl, FlatPlan& P) {
+pgb_status make_plan(pgb_batch* b, int wpb, int filter_pl, int visited_pl, FlatPlan& P) {
     const pgb_index* ix = b->index;
     FlatPlanRequest rq;
     rq.max_ls = b->opt.max_beam;
     rq.deg_lim = b->opt.degree_limit ? std::min(b->opt.degree_limit, ix->G) : ix->G;
     rq.is_signed = ix->elem == PGB_INT8;
     rq.batched = true;
-    rq.queries_per_warp = qpw;
     rq.warps_per_block = wpb;
     if (filter_pl) {
         rq.force_filter_placement = true;
@@ -73,8 +71,8 @@ pgb_status make_plan(pgb_batch* b, int qpw, int wpb, int filter_pl, int visited_
 
 // scratch for the plan's global tables (grown, never shrunk)
 pgb_status ensure_scratch(pgb_batch* b, const FlatPlan& P) {
-    const uint64_t fw = (uint64_t)P.gfilter_words * P.total_slots;
-    const uint64_t vw = (uint64_t)P.gvisited_words * P.total_slots;
+    const uint64_t fw = (uint64_t)P.gfilter_words * P.total_warps;
+    const uint64_t vw = (uint64_t)P.gvisited_words * P.total_warps;
     pgb_status s;
     if (fw > b->gfilter_words) {
         cudaFree(b->gfilter);
@@ -170,8 +168,7 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
     if (opt->max_queries == 0 || opt->max_beam == 0 || opt->max_beam > PGB_MAX_BEAM ||
         opt->max_k == 0 || opt->max_k > PGB_MAX_K || !(opt->cut > 0))
         return fail(PGB_ERR_BAD_ARG, "bad max_queries / max_beam / max_k / cut");
-    if (opt->warps_per_block > 4 || opt->filter_placement > 2 || opt->visited_placement > 2 ||
-        opt->queries_per_warp > 2)
+    if (opt->warps_per_block > 4 || opt->filter_placement > 2 || opt->visited_placement > 2)
         return fail(PGB_ERR_BAD_ARG, "bad launch shape or placement option");
     DeviceGuard guard(ix->device);
     if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
@@ -187,8 +184,7 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
     hp.cut = opt->cut;
     hp.limit = opt->limit;
     if ((s = b->hnsw ? hnsw_prepare(ix, hp, b->hs)
-                     : make_plan(b, opt->queries_per_warp ? (int)opt->queries_per_warp : 1,
-                                 (int)opt->warps_per_block, (int)opt->filter_placement,
+                     : make_plan(b, (int)opt->warps_per_block, (int)opt->filter_placement,
                                  (int)opt->visited_placement, b->plan)) != PGB_OK ||
         (!b->hnsw && (s = ensure_scratch(b, b->plan)) != PGB_OK) ||
         (s = cuda_status(cudaMalloc(&b->d_ls, 4 * nq), "batch arrays")) != PGB_OK ||
@@ -324,22 +320,19 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
         b->tuned_ms = ms / 2;
         return PGB_OK;
     }
-    const int qpws[] = {1, 2};
     const int wpbs[] = {1, 2, 4};
     const int fpls[] = {1, 2};
     const int vpls[] = {1, 2};
     float best = 1e30f;
     FlatPlan best_plan = b->plan;
-    for (int qpw : qpws)
     for (int wpb : wpbs)
         for (int fp : fpls)
             for (int vp : vpls) {
-                if (b->opt.queries_per_warp && (int)b->opt.queries_per_warp != qpw) continue;
                 if (b->opt.warps_per_block && (int)b->opt.warps_per_block != wpb) continue;
                 if (b->opt.filter_placement && (int)b->opt.filter_placement != fp) continue;
                 if (b->opt.visited_placement && (int)b->opt.visited_placement != vp) continue;
                 FlatPlan P;
-                if (make_plan(b, qpw, wpb, fp, vp, P) != PGB_OK) continue;  // does not fit
+                if (make_plan(b, wpb, fp, vp, P) != PGB_OK) continue;  // does not fit
                 if (P.warps_per_block != wpb) continue;
                 if (ensure_scratch(b, P) != PGB_OK) continue;
                 float ms = 0.f, t = 0.f;
@@ -378,16 +371,14 @@ pgb_status pgb_batch_get_config(const pgb_batch* b, pgb_batch_config* out) {
         out->visited_in_shared = 1u;  // is_inw is the workset, in shared memory
         out->shared_bytes_per_warp = b->hs.warp_bytes;
         out->tuned_ms = b->tuned_ms;
-        out->queries_per_warp = 1;
         return PGB_OK;
     }
     out->warps_per_block = (uint32_t)b->plan.warps_per_block;
     out->blocks = (uint32_t)b->plan.blocks;
     out->filter_in_shared = b->plan.sfilt ? 1u : 0u;
     out->visited_in_shared = b->plan.svis ? 1u : 0u;
-    out->shared_bytes_per_warp = b->plan.L.bytes * (uint32_t)b->plan.queries_per_warp;
+    out->shared_bytes_per_warp = b->plan.L.bytes;
     out->tuned_ms = b->tuned_ms;
-    out->queries_per_warp = (uint32_t)b->plan.queries_per_warp;
     return PGB_OK;
 }
 

@@ -98,7 +98,6 @@ extern "C" pgb_status pgb_search_flat_noalloc(const pgb_index* ix, const pgb_que
             if ((uint64_t)np.blocks > fit_blocks) {
                 np.blocks = (int)fit_blocks;
                 np.total_warps = fit_blocks * (uint64_t)np.warps_per_block;
-                np.total_slots = np.total_warps;
             }
             d.plan = np;
             d.ls = p.beam_size;

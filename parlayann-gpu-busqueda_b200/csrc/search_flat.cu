@@ -47,11 +47,6 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     P.ch = flat_chunks_for(rq.deg_lim);
     P.batched = rq.batched;
     P.is_signed = rq.is_signed;
-    if (rq.queries_per_warp != 1 && !(rq.queries_per_warp == 2 && rq.batched))
-        return fail(PGB_ERR_BAD_ARG, "two queries per warp is a batched schedule; otherwise one");
-    P.queries_per_warp = rq.queries_per_warp;
-    const bool pair = P.queries_per_warp == 2;
-    if (pair && P.ch > 4) return fail(PGB_ERR_BAD_ARG, "the paired schedule serves rows of up to 128 neighbours");
     const uint32_t ls = rq.max_ls;
     const uint32_t fwords = 1u << flat_filter_bits(ls);
     const uint32_t vwords = flat_visited_cap(ls);
@@ -70,12 +65,10 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     P.gvisited_words = P.svis ? 0u : vwords;
     const uint32_t kfw = P.sfilt ? fwords : 0u;
     if (rq.codes && rq.batched) return fail(PGB_ERR_BAD_ARG, "code rows are searched by the plain schedule only");
-    const FlatSchedule sched = P.batched ? (pair ? FlatSchedule::kPair : FlatSchedule::kBatched)
+    const FlatSchedule sched = P.batched ? FlatSchedule::kBatched
                                          : (rq.codes ? FlatSchedule::kPlainCodes : FlatSchedule::kPlain);
     P.kernel = pick(P.ch, sched, P.is_signed, kfw);
-    if (P.batched)
-        P.kernel_uniform = pick(P.ch, pair ? FlatSchedule::kPairUniform : FlatSchedule::kBatchedUniform,
-                                P.is_signed, kfw);
+    if (P.batched) P.kernel_uniform = pick(P.ch, FlatSchedule::kBatchedUniform, P.is_signed, kfw);
     if (!P.kernel || (P.batched && !P.kernel_uniform))
         return fail(PGB_ERR_BAD_ARG, "no kernel for this filter size");
 
@@ -86,8 +79,7 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
         return fail(PGB_ERR_CUDA, "cudaGetDeviceProperties failed");
     const size_t smem_cap = prop.sharedMemPerBlockOptin;
     // at most 4 warps per block: the kernels are built for 128 threads, 9 blocks per SM
-    // (the paired kernel: 5); a paired warp holds two query slices
-    const size_t warp_bytes = (size_t)P.queries_per_warp * P.L.bytes;
+    const size_t warp_bytes = P.L.bytes;
     int wpb = rq.warps_per_block > 0 ? std::min(rq.warps_per_block, 4) : 4;
     while (wpb > 1 && (size_t)wpb * warp_bytes > smem_cap) wpb >>= 1;
     if ((size_t)wpb * warp_bytes > smem_cap)
@@ -120,7 +112,6 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P) {
     P.blocks_per_sm = bps;
     P.blocks = bps * prop.multiProcessorCount;
     P.total_warps = (uint64_t)P.blocks * wpb;
-    P.total_slots = P.total_warps * (uint64_t)P.queries_per_warp;
     return PGB_OK;
 }
 
@@ -131,10 +122,8 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream, const
     void* args[] = {&A};
     // the work-queue form needs no more warps than queries (small serving batches)
     int blocks = P.blocks;
-    if (P.batched) {
-        const uint32_t per_block = (uint32_t)(P.warps_per_block * P.queries_per_warp);
-        blocks = std::max(1, std::min(blocks, (int)((A.nq + per_block - 1) / per_block)));
-    }
+    if (P.batched)
+        blocks = std::max(1, std::min(blocks, (int)((A.nq + P.warps_per_block - 1) / P.warps_per_block)));
     void* kern = (P.batched && !A.ls_arr) ? P.kernel_uniform : P.kernel;
     cudaError_t e;
     if (ix && ix->l2_bytes) {

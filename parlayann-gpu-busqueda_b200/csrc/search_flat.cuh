@@ -153,9 +153,8 @@ __host__ __device__ constexpr FlatLayout make_flat_layout(uint32_t ls_cap, uint3
 
 // plain: static query striding; batched: device work queue with per-query (Ls, k);
 // batched uniform: work queue, one (Ls, k) for the whole launch; plain codes: the plain
-// schedule over 4-bit code rows; pair / pair uniform: the batched forms with two queries
-// per warp (search_flat_pair.cuh)
-enum class FlatSchedule { kPlain, kBatched, kBatchedUniform, kPlainCodes, kPair, kPairUniform };
+// schedule over 4-bit code rows
+enum class FlatSchedule { kPlain, kBatched, kBatchedUniform, kPlainCodes };
 
 struct FlatArgs {
     const uint8_t* rows;   // n x 128-byte vector rows

@@ -7,12 +7,9 @@
 // batched : persistent grid whose warps pull queries from a device counter over a
 //           longest-beam-first order, each query with its own Ls and k; tables sized
 //           for the batch's largest Ls. Same per-query code, identical neighbours.
-// pair    : the batched form with two queries per warp, one on each 16-lane half
-//           (search_flat_pair.cuh); same integers and order, identical neighbours.
 #pragma once
 
 #include "search_flat.cuh"
-#include "search_flat_pair.cuh"
 
 // resident 128-thread blocks per SM the flat kernels are compiled for (registers per
 // thread = 65536 / (128 * this)): 9 -> 56 registers, 36 warps per SM
@@ -91,38 +88,12 @@ __global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_batched_kernel(FlatA
     PGB_PROF_EXIT();
 }
 
-// Paired schedule (batched form only): two queries per warp, one per 16-lane half, each
-// with its own shared-memory slice (2 * A.L.bytes per warp) and global table slot
-// (2 per warp). Rows of up to 128 neighbours (CH <= 4).
-#ifndef PGB_PAIR_MIN_BLOCKS
-#define PGB_PAIR_MIN_BLOCKS 5
-#endif
-template <int CH, bool Signed, int FW, bool UNI>
-__global__ void __launch_bounds__(128, PGB_PAIR_MIN_BLOCKS) flat_pair_kernel(FlatArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    const int half = lane >> 4;
-    const uint32_t wpb = blockDim.x >> 5;
-    const uint32_t qslot = (blockIdx.x * wpb + w) * 2u + (uint32_t)half;
-    unsigned char* wmem = smem + (size_t)(w * 2 + half) * A.L.bytes;
-    uint32_t* gf = A.gfilter ? A.gfilter + (size_t)qslot * A.gfilter_words : nullptr;
-    uint32_t* gv = A.gvisited ? A.gvisited + (size_t)qslot * A.gvisited_words : nullptr;
-    flat_pair_run<CH, Signed, FW, UNI>(A, wmem, gf, gv, lane);
-}
-
 template <int CH, bool Signed, int FW>
 void* flat_kernel_of(FlatSchedule sched) {
     switch (sched) {
         case FlatSchedule::kPlain: return (void*)flat_plain_kernel<CH, Signed, FW>;
         case FlatSchedule::kBatched: return (void*)flat_batched_kernel<CH, Signed, FW, false>;
         case FlatSchedule::kPlainCodes: return (void*)flat_plain_kernel<CH, Signed, FW, true>;
-        case FlatSchedule::kPair:
-            if constexpr (CH <= 4) return (void*)flat_pair_kernel<CH, Signed, FW, false>;
-            else return nullptr;
-        case FlatSchedule::kPairUniform:
-            if constexpr (CH <= 4) return (void*)flat_pair_kernel<CH, Signed, FW, true>;
-            else return nullptr;
         default: return (void*)flat_batched_kernel<CH, Signed, FW, true>;
     }
 }

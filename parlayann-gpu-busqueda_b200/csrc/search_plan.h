@@ -15,7 +15,6 @@ struct FlatPlanRequest {
     uint32_t deg_lim = 32;         // adjacency entries read per row
     bool is_signed = true;
     bool batched = false;
-    int queries_per_warp = 1;      // batched: 1 (one query per warp) or 2 (paired halves)
     bool codes = false;            // plain schedule over 4-bit code rows (not batched)
     int warps_per_block = 0;       // 0: default (4)
     int max_blocks_per_sm = 0;     // 0: as many as fit
@@ -35,10 +34,8 @@ struct FlatPlan {
     bool batched = false, is_signed = true, sfilt = true, svis = true;
     FlatLayout L{};
     uint32_t gfilter_words = 0, gvisited_words = 0;  // per warp, 0 when in shared memory
-    int queries_per_warp = 1;        // 2: the paired schedule (batched only)
     int warps_per_block = 4, blocks_per_sm = 1, blocks = 1;
     uint64_t total_warps = 0;
-    uint64_t total_slots = 0;        // query slots (shared slices, global tables) = warps * qpw
     size_t smem_bytes = 0;
     void* kernel = nullptr;          // plain, or batched with per-query (Ls, k)
     void* kernel_uniform = nullptr;  // batched: one (Ls, k) for every query
@@ -46,7 +43,7 @@ struct FlatPlan {
 
 int flat_chunks_for(uint32_t deg_lim);
 pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P);
-// A's table pointers must cover P.total_slots slices when the plan keeps them global.
+// A's table pointers must cover P.total_warps slices when the plan keeps them global.
 // A batched launch with A.ls_arr == nullptr runs the uniform kernel on (A.Ls, A.k).
 // ix (optional): the index whose L2 access-policy window, when set, the launch carries.
 pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream,
