@@ -37,6 +37,7 @@ K = 10
 R, L_BUILD, ALPHA = 64, 128, 1.2
 TARGET_RECALL = 0.90
 POLL_HEAD = 4096  # serving client: outstanding tickets polled per pass, oldest first
+PARITY_SAMPLE = 1024  # queries of each full-size parity check against the oracle
 METRIC = "QPS @ recall@10=0.90, batched vs plain kernel, 1 B200; serving p50/p99 latency"
 
 
@@ -48,6 +49,22 @@ def data_dir():
     d = os.environ.get("PGB_DATA", os.path.join(ROOT, "_data"))
     os.makedirs(d, exist_ok=True)
     return d
+
+
+def standalone(name):
+    """A numpy-only module of the package (formats, synthetic) loaded by itself, without
+    importing the package (which maps lib/libpgb.so): the reference arm reads the data
+    files with these and runs only the CPU restatement."""
+    import importlib.util
+    key = "pgb_standalone_" + name
+    if key in sys.modules:
+        return sys.modules[key]
+    spec = importlib.util.spec_from_file_location(
+        key, os.path.join(ROOT, "parlayann-gpu-busqueda_b200", name + ".py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[key] = mod
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def dist_env():
@@ -216,19 +233,39 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def prepare_data(args):
+    """--prepare: the 1M base, rank 0's queries' ground truth and the Vamana graph, built
+    and cached on disk (the reference arm runs this in a separate, untimed process)."""
+    import torch
+    torch.cuda.set_device(0)
+    pgb = ge.load_package()
+    base, queries, _ = load_workload(pgb, 0, lambda: None)
+    ground_truth(base, queries, 0, 0)
+
+
 def run_reference(args, rank):
-    """CPU restatement of the reference search (oracle) on the host cores."""
+    """CPU restatement of the reference search (oracle) on the host cores. This process
+    reads the data with the package's numpy-only readers and never maps the library; a
+    cold data cache is filled first by `bench.py --prepare` in a child process."""
     if rank != 0:
         return
-    pgb = ge.load_package()
-    oracle = ge.load_oracle()
-    base, queries, graph = load_workload(pgb, 0, lambda: None)
+    fmt, syn = standalone("formats"), standalone("synthetic")
+    base_p = os.path.join(data_dir(), "c2_base.i8bin")
+    graph_p = os.path.join(data_dir(), GRAPHS["vamana"][0])
     gt_p = os.path.join(data_dir(), "c2_gt100_q0.bin")
+    if not (os.path.exists(base_p) and os.path.exists(graph_p) and os.path.exists(gt_p)):
+        t = time.time()
+        subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--prepare"], check=True)
+        log(f"data prepared in {time.time() - t:.1f} s (separate process, untimed)")
+    oracle = ge.load_oracle()
+    base = fmt.read_vectors(base_p)
+    graph = fmt.read_graph(graph_p)
+    queries = syn.LAW_C2.sample(N_QUERIES, 0, 1)
     Ls = int(os.environ.get("PGB_REF_LS", "0"))
-    from parlayann_gpu_busqueda_b200 import formats
+    formats = fmt
     if not Ls:
         # same rule as our arm: smallest sweep beam reaching the target recall
-        from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
+        LS_SWEEP = syn.LS_SWEEP
         gi, gd = formats.read_gt(gt_p) if os.path.exists(gt_p) else (None, None)
         Ls = 40
         if gi is not None:
@@ -249,16 +286,18 @@ def run_reference(args, rank):
         t = time.perf_counter()
         oracle.flat_search(base, graph.degrees, graph.edges, q, K, Ls, threads=threads)
         times.append(time.perf_counter() - t)
-    qps = sample * len(times) / sum(times)
+    # the reference's protocol (comparacion1.cu:76-101): warm-up, then the best step
+    qps = sample / min(times)
     line = {
         "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "ms_per_step": 1e3 * min(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
         "config": {"workload": "1M int8 d=100 Vamana R64 L128 a1.2, k=10", "Ls": Ls,
-                   "queries_per_step": sample},
+                   "queries_per_step": sample, "mean_step_qps": sample * len(times) / sum(times)},
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}"},
+                         "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}",
+                         "protocol": f"{args.warmup} warm-up steps, then the best of {args.steps}"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -361,6 +400,128 @@ def run_profile(args, local):
                       "row_stride": (int(index.info.max_degree) + 31) // 32 * 32}))
 
 
+def oracle_agrees(oracle, base, kind, graph, queries, Ls, got):
+    """True when the oracle's ids, int32 distances, distance counts, expansions and flags
+    equal `got` = (ids, dists, stats) of the first PARITY_SAMPLE queries at beam Ls."""
+    qs = np.ascontiguousarray(queries[:PARITY_SAMPLE])
+    o = (oracle.hnsw_search(base, graph, qs, K, Ls) if kind == "hnsw"
+         else oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls))
+    ids, dists, st = got
+    return bool(np.array_equal(ids, o[0]) and np.array_equal(dists, o[1]) and
+                np.array_equal(st[:, 0], o[2]) and np.array_equal(st[:, 1], o[3]) and
+                np.array_equal(st[:, 2], o[4]))
+
+
+def run_extras(args, pgb, torch, dev, local, base, queries, graph, gt_ids, gt_d, oracle, flush,
+               Ls, swept):
+    """After the headline, on one GPU: (1) full-size parity against the oracle on the first
+    PARITY_SAMPLE queries -- Vamana at the smallest, the operating, the widest swept beam and
+    at 316 (global filter and visited tables), and HCNNG, PyNNDescent and HNSW at their own
+    recall@10 >= 0.90 beams; (2) those families' plain and batched QPS with the L2 flushed
+    and their gather roofline; (3) the serving loop on the Vamana graph and the HNSW model
+    at two offered rates. Returns the three blocks of the bench line."""
+    from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
+    t_start = time.time()
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    q_dev = torch.from_numpy(queries.view(np.uint8)).to(dev)
+    peak, _ = measured_peaks()
+    ident = {}
+    for ls in sorted({LS_SWEEP[0], Ls, max(swept)}):
+        ident[f"vamana Ls={ls}"] = oracle_agrees(oracle, base, "vamana", graph, queries, ls, swept[ls])
+    index = pgb.Index.flat(base, graph, device=local)
+    wide = 316
+    s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=wide))
+    wi, wd, ws = s.search_device(q_dev, sp)
+    b = pgb.Batch(index, N_QUERIES, max_beam=wide, max_k=K)
+    b.plan(np.full(N_QUERIES, wide, np.uint32), np.full(N_QUERIES, K, np.uint32))
+    bi, bd, bs = b.outputs(dev)
+    b.search(q_dev, bi, bd, bs, sp)
+    torch.cuda.synchronize(dev)
+    ident[f"vamana Ls={wide}"] = (
+        oracle_agrees(oracle, base, "vamana", graph, queries, wide,
+                      (wi.cpu().numpy().view(np.uint32)[:PARITY_SAMPLE],
+                       wd.cpu().numpy()[:PARITY_SAMPLE], ws.cpu().numpy()[:PARITY_SAMPLE]))
+        and bool(torch.equal(wi, bi) and torch.equal(wd, bd)))
+    s.liberar()
+    b.close()
+    index.close()
+
+    families = {}
+    for kind in ("hcnng", "nnd", "hnsw"):
+        t0 = time.time()
+        if kind == "hnsw":
+            _, fg = load_hnsw(pgb)
+            index = pgb.Index.hnsw(base, fg, device=local)
+        else:
+            _, _, fg = load_workload(pgb, 0, lambda: None, kind)
+            index = pgb.Index.flat(base, fg, device=local)
+        setup_s = time.time() - t0
+        fam_ls, sweep, kept = None, [], None
+        for ls in LS_SWEEP:
+            s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=ls))
+            ids, dists, st = s.search_device(q_dev, sp)
+            torch.cuda.synchronize(dev)
+            ids_h = ids.cpu().numpy().view(np.uint32)
+            rec = pgb.recall(gt_ids, gt_d, ids_h, K)
+            sweep.append([ls, round(rec, 5)])
+            s.liberar()
+            if rec >= TARGET_RECALL or ls == LS_SWEEP[-1]:
+                fam_ls = ls
+                kept = (ids_h[:PARITY_SAMPLE], dists.cpu().numpy()[:PARITY_SAMPLE],
+                        st.cpu().numpy()[:PARITY_SAMPLE])
+                break
+        ident[f"{kind} Ls={fam_ls}"] = oracle_agrees(oracle, base, kind, fg, queries, fam_ls, kept)
+        plain = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=fam_ls))
+        p_ids = torch.empty((N_QUERIES, K), dtype=torch.int32, device=dev)
+        p_d = torch.empty_like(p_ids)
+        p_st = torch.empty((N_QUERIES, 4), dtype=torch.int32, device=dev)
+        tp = _timed_events(torch, stream, lambda: plain.lanzar(q_dev, p_ids, p_d, p_st, sp),
+                           args.steps, args.warmup, flush)
+        b = pgb.Batch(index, N_QUERIES, max_beam=fam_ls, max_k=K)
+        b.plan(np.full(N_QUERIES, fam_ls, np.uint32), np.full(N_QUERIES, K, np.uint32))
+        bi, bd, bs = b.outputs(dev)
+        cfg = b.tune(q_dev, bi, bd, bs)
+        b.capture(q_dev, bi, bd, bs)
+        tb = _timed_events(torch, stream, lambda: b.replay(sp), args.steps, args.warmup, flush)
+        stn = p_st.cpu().numpy()
+        gsz = (int(index.info.max_degree) + 31) // 32 * 32
+        bytes_launch = float(128 * stn[:, 0].astype(np.int64).sum() +
+                             4 * gsz * stn[:, 1].astype(np.int64).sum())
+        mp, mb = sum(tp) / len(tp) / 1e3, sum(tb) / len(tb) / 1e3
+        families[kind] = {
+            "graph": GRAPHS[kind][1] if kind != "hnsw" else "HNSW M32 efc128",
+            "Ls": fam_ls, "recall_at_10": dict((a, c) for a, c in sweep)[fam_ls],
+            "plain_qps": N_QUERIES / mp, "batched_qps": N_QUERIES / mb,
+            "batched_over_plain": mp / mb,
+            "identical_neighbours": bool(torch.equal(p_ids, bi) and torch.equal(p_d, bd)),
+            "frac": bytes_launch / mb / 1e9 / peak, "plain_frac": bytes_launch / mp / 1e9 / peak,
+            "kernel": "hnsw_kernel" if kind == "hnsw" else "flat_batched_kernel",
+            "comps_per_query": float(stn[:, 0].mean()),
+            "expansions_per_query": float(stn[:, 1].mean()),
+            "batched_config": cfg, "setup_s": round(setup_s, 1)}
+        log(kind, families[kind])
+        plain.liberar()
+        b.close()
+        index.close()
+
+    serving = {}
+    rng = np.random.default_rng(1)
+    seconds = float(os.environ.get("PGB_SERVE_SECONDS", "2"))
+    for kind in ("vamana", "hnsw"):
+        if kind == "hnsw":
+            _, h = load_hnsw(pgb)
+            index = pgb.Index.hnsw(base, h, device=local)
+        else:
+            index = pgb.Index.flat(base, graph, device=local)
+        serving[kind] = [serve_rate(pgb, index, queries, gt_ids, gt_d, rate, seconds, rng)
+                         for rate in (100_000, 1_000_000)]
+        log("serving", kind, serving[kind])
+        index.close()
+    log(f"extras in {time.time() - t_start:.1f} s")
+    return {"identical_to_oracle": ident, "families": families, "serving": serving}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -368,6 +529,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: skip the other graph families' parity / QPS and the "
+                         "serving leg (always skipped with more than one GPU)")
+    ap.add_argument("--prepare", action="store_true",
+                    help="build and cache the headline data (base, graph, ground truth), then exit")
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: the 1M index, --profile-nq queries at --profile-ls, "
                          "warm-up then --steps launches of each kernel, nothing else")
@@ -389,6 +555,9 @@ def main():
                          "vs vector rows, plain kernel, 1M Vamana")
     args = ap.parse_args()
     rank, world, local = dist_env()
+    if args.prepare:
+        prepare_data(args)
+        return
     if args.profile:
         if args.workload == "hnsw":
             run_profile_hnsw(args, local)
@@ -431,13 +600,17 @@ def main():
     sp = stream.cuda_stream
 
     # ---- operating point: smallest sweep beam with recall@10 >= 0.90 ---------------
-    sweep, Ls = [], None
+    # (the first PARITY_SAMPLE rows of every swept beam are kept for the oracle check)
+    sweep, Ls, swept = [], None, {}
     for ls in LS_SWEEP:
         s = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=ls))
         ids, dists, st = s.search_device(q_dev, sp)
         torch.cuda.synchronize(dev)
-        rec = pgb.recall(gt_ids, gt_d, ids.cpu().numpy().view(np.uint32), K)
+        ids_h = ids.cpu().numpy().view(np.uint32)
+        rec = pgb.recall(gt_ids, gt_d, ids_h, K)
         sweep.append([ls, round(rec, 5)])
+        swept[ls] = (ids_h[:PARITY_SAMPLE], dists.cpu().numpy()[:PARITY_SAMPLE],
+                     st.cpu().numpy()[:PARITY_SAMPLE])
         s.liberar()
         if rec >= TARGET_RECALL and Ls is None:
             Ls = ls
@@ -450,11 +623,14 @@ def main():
     # L2 flush between timed steps (a write larger than the 126 MB L2)
     flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
 
+    launches = [0]  # search kernels launched inside the timed steps (the library's counter)
+
     def timed(fn, steps, warmup):
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize(dev)
         ev = []
+        c0 = pgb.search_launches()
         for _ in range(steps):
             flush.fill_(1)
             barrier()
@@ -466,6 +642,7 @@ def main():
             torch.cuda.synchronize(dev)
             barrier()
             ev.append(a.elapsed_time(b))
+        launches[0] += pgb.search_launches() - c0
         return ev
 
     # ---- plain warp-per-query kernel (the drop-in) ----------------------------------
@@ -503,6 +680,7 @@ def main():
     for _ in range(args.warmup):
         run_e2e()
     e2e_t = []
+    c0 = pgb.search_launches()
     for _ in range(args.steps):
         flush.fill_(1)
         torch.cuda.synchronize(dev)
@@ -511,6 +689,7 @@ def main():
         run_e2e()
         e2e_t.append(time.perf_counter() - t)
         barrier()
+    launches[0] += pgb.search_launches() - c0
     clk.__exit__(None, None, None)
     clocks = clk.summary()
     e2e_ok = bool(np.array_equal(e_ids.numpy(), p_ids.cpu().numpy()))
@@ -564,6 +743,14 @@ def main():
                         "sample": f"first {sample} of {N_QUERIES} queries at Ls={Ls}, best of 5",
                         "one_thread_qps": one, "cpu_model": cpu_model()}
 
+    # ---- beyond the headline (one GPU): oracle parity of every graph family at full size,
+    # their QPS and gather roofline, and the serving loop's latency ------------------------
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        oracle = ge.load_oracle()
+        extras = run_extras(args, pgb, torch, dev, local, base, queries, graph, gt_ids, gt_d,
+                            oracle, flush, Ls, swept)
+
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -604,8 +791,14 @@ def main():
                          "expansions_per_query": float(st[:, 1].mean())},
             "cpu_baseline": cpu_baseline,
             "clocks": clocks,
-            "gpu_launches": 3 * args.steps,  # one search kernel per step in each of 3 arms
+            # counted by the library: search kernels launched in the timed steps of the
+            # plain, batched (graph replays) and end-to-end arms
+            "gpu_launches": int(launches[0]),
         }
+        if extras:
+            line["config"]["identical_to_oracle"] = extras["identical_to_oracle"]
+            line["families"] = extras["families"]
+            line["serving"] = extras["serving"]
         print(json.dumps(line), flush=True)
     plain.liberar()
     batch.close()
@@ -615,11 +808,17 @@ def main():
         dist.destroy_process_group()
 
 
+# search kernels the library launched inside _timed_events' timed steps, for gpu_launches
+_TIMED_LAUNCHES = [0]
+
+
 def _timed_events(torch, stream, fn, steps, warmup, flush=None):
+    pgb = ge.load_package()
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
     out = []
+    c0 = pgb.search_launches()
     for _ in range(steps):
         if flush is not None:
             flush.fill_(1)
@@ -630,6 +829,7 @@ def _timed_events(torch, stream, fn, steps, warmup, flush=None):
         b.record(stream)
         torch.cuda.synchronize()
         out.append(a.elapsed_time(b))
+    _TIMED_LAUNCHES[0] += pgb.search_launches() - c0
     return out
 
 
@@ -685,7 +885,7 @@ def run_hnsw(args, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_source": kind,
                      "kernel": "hnsw_kernel"},
-        "gpu_launches": args.steps}), flush=True)
+        "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
 
 
 def run_codes(args, local):
@@ -771,7 +971,7 @@ def run_codes(args, local):
         "roofline": {"bound": "hbm", "achieved": c["algorithmic_gb_per_s"], "peak": peak,
                      "unit": "GB/s", "frac": c["frac_of_hbm_peak"], "traffic": None,
                      "peak_source": kind, "kernel": "flat_plain_kernel (code rows) + rerank_kernel"},
-        "gpu_launches": 2 * args.steps}), flush=True)
+        "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
 
 
 def run_build(args, local):
@@ -888,6 +1088,8 @@ def run_c4(args, local):
     flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
     peak, kind = measured_peaks()
     gs = (int(index.info.max_degree) + 31) // 32 * 32
+    oracle = ge.load_oracle()
+    c4_sample = 512  # queries of the oracle check at every beam
     rows = []
     for ls in C4_LS:
         s = pgb.Searcher(index, C4_NQ, pgb.QueryParams(k=K, beam_size=ls))
@@ -904,12 +1106,21 @@ def run_c4(args, local):
         tb = _timed_events(torch, stream, lambda: b.replay(sp), args.steps, args.warmup, flush)
         identical = bool(torch.equal(ids, bi) and torch.equal(d, bd))
         stn = st.cpu().numpy()
-        rec = pgb.recall(gt_ids, gt_d, ids.cpu().numpy().view(np.uint32), K)
+        ids_h = ids.cpu().numpy().view(np.uint32)
+        rec = pgb.recall(gt_ids, gt_d, ids_h, K)
+        o = oracle.flat_search(base, graph.degrees, graph.edges,
+                               np.ascontiguousarray(queries[:c4_sample]), K, ls)
+        same_oracle = bool(np.array_equal(ids_h[:c4_sample], o[0]) and
+                           np.array_equal(d.cpu().numpy()[:c4_sample], o[1]) and
+                           np.array_equal(stn[:c4_sample, 0], o[2]) and
+                           np.array_equal(stn[:c4_sample, 1], o[3]) and
+                           np.array_equal(stn[:c4_sample, 2], o[4]))
         bytes_launch = float(128 * stn[:, 0].astype(np.int64).sum() + 4 * gs * stn[:, 1].astype(np.int64).sum())
         mb = sum(tb) / len(tb) / 1e3
         rows.append({"Ls": ls, "recall_at_10": round(rec, 5),
                      "plain_qps": C4_NQ * len(tp) / (sum(tp) / 1e3),
                      "batched_qps": C4_NQ / mb, "identical_neighbours": identical,
+                     "identical_to_oracle": same_oracle, "oracle_sample": c4_sample,
                      "comps_per_query": float(stn[:, 0].mean()),
                      "expansions_per_query": float(stn[:, 1].mean()),
                      "achieved_gbs": bytes_launch / mb / 1e9,
@@ -933,7 +1144,7 @@ def run_c4(args, local):
         "roofline": {"bound": "hbm", "achieved": head["achieved_gbs"], "peak": peak, "unit": "GB/s",
                      "frac": head["frac"], "traffic": None, "peak_source": kind,
                      "kernel": "flat_batched_kernel"},
-        "gpu_launches": 2 * args.steps * len(rows)}), flush=True)
+        "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
 
 
 def run_mixed(args, local, kind="vamana"):
@@ -1005,7 +1216,69 @@ def run_mixed(args, local, kind="vamana"):
                    "plain_timing": "sum of per-group launch times (events), L2 warm",
                    "identical_neighbours": bool(same), "batched_config": tuned,
                    "l2": "flushed before every timed step"},
-        "gpu_launches": steps + len(plain)}), flush=True)
+        "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
+
+
+def serve_rate(pgb, index, queries, gt_ids, gt_d, rate, seconds, rng):
+    """One offered rate through the request loop for `seconds`: Poisson arrival events,
+    half single queries and half bursts of 2-256, per-request Ls in {20,50,100,300} and k
+    in {10,100}; sustained QPS, the server's p50/p99 submit-to-completion latency, the
+    refused fraction and recall@10 of the completed requests."""
+    srv = pgb.Server(index, max_beam=300, max_k=100, max_batch=2048, max_inflight=4)
+    # arrival events: half single queries, half bursts uniform in 2..256
+    mean_burst = 0.5 * 1 + 0.5 * 129
+    n_events = max(1, int(rate * seconds / mean_burst))
+    gaps = rng.exponential(mean_burst / rate, n_events)
+    sizes = np.where(rng.random(n_events) < 0.5, 1, rng.integers(2, 257, n_events))
+    t_evt = np.cumsum(gaps)
+    # every request's query, beam and k drawn before the clock starts: event e submits
+    # rows off[e]:off[e+1] of these arrays (contiguous views, no copies in the loop)
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    sel_all = rng.integers(0, N_QUERIES, int(off[-1]))
+    q_all = np.ascontiguousarray(queries[sel_all])
+    L_all = rng.choice(np.array([20, 50, 100, 300], np.uint32), int(off[-1]))
+    k_all = rng.choice(np.array([10, 100], np.uint32), int(off[-1]))
+    # outstanding tickets in submission order; each pass polls the oldest POLL_HEAD of
+    # them (batches complete roughly in launch order), so the client's own work stays
+    # bounded when the server is saturated and the pool holds thousands of requests
+    out_t, out_q = np.empty(0, np.uint64), np.empty(0, np.int64)
+    new_t, new_q = [], []
+    issued, done_q, recalls = 0, 0, []
+    t0 = time.perf_counter()
+    ev = 0
+    while ev < n_events or len(out_t) or new_t:
+        now = time.perf_counter() - t0
+        while ev < n_events and t_evt[ev] <= now:
+            a, b = int(off[ev]), int(off[ev + 1])
+            t = srv.submit_many(q_all[a:b], L_all[a:b], k_all[a:b])
+            if len(t):
+                new_t.append(t)
+                new_q.append(sel_all[a:a + len(t)])
+            issued += len(t)
+            ev += 1
+        if new_t:
+            out_t = np.concatenate([out_t] + new_t)
+            out_q = np.concatenate([out_q] + new_q)
+            new_t, new_q = [], []
+        if len(out_t):
+            head_t, head_q = out_t[:POLL_HEAD], out_q[:POLL_HEAD]
+            done, oi, _, _ = srv.poll_many(head_t)
+            if done.any():
+                rec = pgb.recall(gt_ids[head_q[done]], gt_d[head_q[done]], oi[done][:, :K], K)
+                recalls.append((rec, int(done.sum())))
+                done_q += int(done.sum())
+                out_t = np.concatenate([head_t[~done], out_t[POLL_HEAD:]])
+                out_q = np.concatenate([head_q[~done], out_q[POLL_HEAD:]])
+        if now > 20 * seconds:
+            break
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    rec = sum(r * n for r, n in recalls) / max(1, sum(n for _, n in recalls))
+    return {"offered_qps": rate, "sustained_qps": done_q / wall, "p50_us": st["p50_us"],
+            "p99_us": st["p99_us"], "rejected": st["rejected"],
+            "refused_frac": st["rejected"] / max(1, st["rejected"] + issued),
+            "launches": st["launches"], "mean_batch": st["mean_batch"], "recall_at_10": rec}
 
 
 def run_serving(args, local, kind="vamana"):
@@ -1029,60 +1302,7 @@ def run_serving(args, local, kind="vamana"):
     seconds = float(os.environ.get("PGB_SERVE_SECONDS", "1.5"))
     rows = []
     for rate in rates:
-        srv = pgb.Server(index, max_beam=300, max_k=100, max_batch=2048, max_inflight=4)
-        # arrival events: half single queries, half bursts uniform in 2..256
-        mean_burst = 0.5 * 1 + 0.5 * 129
-        n_events = max(1, int(rate * seconds / mean_burst))
-        gaps = rng.exponential(mean_burst / rate, n_events)
-        sizes = np.where(rng.random(n_events) < 0.5, 1, rng.integers(2, 257, n_events))
-        t_evt = np.cumsum(gaps)
-        # every request's query, beam and k drawn before the clock starts: event e submits
-        # rows off[e]:off[e+1] of these arrays (contiguous views, no copies in the loop)
-        off = np.concatenate([[0], np.cumsum(sizes)])
-        sel_all = rng.integers(0, N_QUERIES, int(off[-1]))
-        q_all = np.ascontiguousarray(queries[sel_all])
-        L_all = rng.choice(np.array([20, 50, 100, 300], np.uint32), int(off[-1]))
-        k_all = rng.choice(np.array([10, 100], np.uint32), int(off[-1]))
-        # outstanding tickets in submission order; each pass polls the oldest POLL_HEAD of
-        # them (batches complete roughly in launch order), so the client's own work stays
-        # bounded when the server is saturated and the pool holds thousands of requests
-        out_t, out_q = np.empty(0, np.uint64), np.empty(0, np.int64)
-        new_t, new_q = [], []
-        issued, done_q, recalls = 0, 0, []
-        t0 = time.perf_counter()
-        ev = 0
-        while ev < n_events or len(out_t) or new_t:
-            now = time.perf_counter() - t0
-            while ev < n_events and t_evt[ev] <= now:
-                a, b = int(off[ev]), int(off[ev + 1])
-                t = srv.submit_many(q_all[a:b], L_all[a:b], k_all[a:b])
-                if len(t):
-                    new_t.append(t)
-                    new_q.append(sel_all[a:a + len(t)])
-                issued += len(t)
-                ev += 1
-            if new_t:
-                out_t = np.concatenate([out_t] + new_t)
-                out_q = np.concatenate([out_q] + new_q)
-                new_t, new_q = [], []
-            if len(out_t):
-                head_t, head_q = out_t[:POLL_HEAD], out_q[:POLL_HEAD]
-                done, oi, _, _ = srv.poll_many(head_t)
-                if done.any():
-                    rec = pgb.recall(gt_ids[head_q[done]], gt_d[head_q[done]], oi[done][:, :K], K)
-                    recalls.append((rec, int(done.sum())))
-                    done_q += int(done.sum())
-                    out_t = np.concatenate([head_t[~done], out_t[POLL_HEAD:]])
-                    out_q = np.concatenate([head_q[~done], out_q[POLL_HEAD:]])
-            if now > 20 * seconds:
-                break
-        wall = time.perf_counter() - t0
-        st = srv.stats()
-        srv.close()
-        rec = sum(r * n for r, n in recalls) / max(1, sum(n for _, n in recalls))
-        rows.append({"offered_qps": rate, "sustained_qps": done_q / wall, "p50_us": st["p50_us"],
-                     "p99_us": st["p99_us"], "rejected": st["rejected"], "launches": st["launches"],
-                     "mean_batch": st["mean_batch"], "recall_at_10": rec})
+        rows.append(serve_rate(pgb, index, queries, gt_ids, gt_d, rate, seconds, rng))
         log(rows[-1])
     best = max(rows, key=lambda r: r["sustained_qps"])
     print(json.dumps({

@@ -345,6 +345,11 @@ pgb_status pgb_server_destroy(pgb_server* s);
 double pgb_recall(const uint32_t* gt_ids, const float* gt_dists, uint32_t nq, uint32_t gt_k,
                   const uint32_t* ids, uint32_t k);
 
+/* Search kernels (flat, HNSW, re-rank, pair distances) this process has launched through
+ * the library so far, each replay of a captured batch graph counting its kernels: a host
+ * counter for checking how many launches a timed region made. */
+uint64_t pgb_search_launches(void);
+
 /* ---- section profiler ----------------------------------------------------------------
  * In a library built with the section profiler (libpgb_prof.so), each flat-search warp adds
  * the clock cycles of every search phase to device totals (the reference's -DPERFIL

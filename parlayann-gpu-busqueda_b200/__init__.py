@@ -9,12 +9,12 @@ from .formats import (Graph, Hnsw, read_graph, read_gt, read_hnsw, read_vectors,
                       write_gt, write_hnsw, write_vectors)
 from .search import (Batch, Index, QueryParams, Searcher, Server, build_hcnng, build_hcnng_gpu, build_hnsw,
                      build_nndescent, build_hnsw_gpu, build_vamana, build_vamana_gpu, device_available,
-                     file_check, recall)
+                     file_check, recall, search_launches)
 
 __all__ = [
     "PgbError", "NO_NEIGHBOR", "FLAG_OVERFLOW", "FLAG_SHORT", "Graph", "Hnsw", "read_graph",
     "read_gt", "read_hnsw", "read_vectors", "write_graph", "write_gt", "write_hnsw",
     "write_vectors", "Batch", "Index", "Server", "QueryParams", "Searcher", "build_hcnng",
     "build_hcnng_gpu", "build_hnsw", "build_nndescent", "build_hnsw_gpu", "build_vamana",
-    "build_vamana_gpu", "device_available", "file_check", "recall",
+    "build_vamana_gpu", "device_available", "file_check", "recall", "search_launches",
 ]

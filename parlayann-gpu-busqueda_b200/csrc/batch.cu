@@ -39,6 +39,7 @@ struct pgb_batch {
     uint32_t uniform_ls = 0, uniform_k = 0;  // the plan's (Ls, k) when all queries share it
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    int64_t graph_launches = 0;  // search kernels in the captured graph
     // host-memory path staging
     uint8_t* q_dev = nullptr;
     uint32_t* ids_dev = nullptr;
@@ -398,7 +399,12 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
         return s;
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
+        // launches made during the capture only record graph nodes: they count once per
+        // replay instead
+        const int64_t before = (int64_t)pgb_search_launches();
         pgb_status ls = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
+        b->graph_launches = (int64_t)pgb_search_launches() - before;
+        count_launches(-b->graph_launches);
         cudaGraph_t g = nullptr;
         e = cudaStreamEndCapture(st, &g);
         if (ls != PGB_OK) {
@@ -423,7 +429,9 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
 pgb_status pgb_batch_replay(pgb_batch* b, void* stream) {
     if (!b || !b->graph_exec) return fail(PGB_ERR_BAD_ARG, "no captured graph");
     DeviceGuard guard(b->index->device);
-    return cuda_status(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream), "graph launch");
+    const pgb_status s = cuda_status(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream), "graph launch");
+    if (s == PGB_OK) count_launches(b->graph_launches);
+    return s;
 }
 
 pgb_status pgb_batch_destroy(pgb_batch* b) {

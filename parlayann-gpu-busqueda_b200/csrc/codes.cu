@@ -15,6 +15,7 @@
 #include "errors.h"
 #include "index.h"
 #include "search_flat.cuh"
+#include "search_plan.h"
 
 namespace pgb {
 namespace {
@@ -224,6 +225,7 @@ pgb_status rerank_launch(const pgb_index* ix, const void* queries, uint32_t nq,
     const unsigned blocks = (unsigned)std::min<uint64_t>((nq + wpb - 1) / wpb, (uint64_t)sms * 8);
     void* args[] = {&A};
     e = cudaLaunchKernel(kern, dim3(blocks), dim3(wpb * 32), args, smem, stream);
+    if (e == cudaSuccess) count_launches(1);
     return e == cudaSuccess ? PGB_OK : cuda_error(e, "re-rank launch");
 }
 

@@ -10,6 +10,7 @@
 #include "errors.h"
 #include "index.h"
 #include "search_flat.cuh"
+#include "search_plan.h"
 #include "searcher.h"
 
 namespace pgb {
@@ -111,6 +112,7 @@ extern "C" pgb_status pgb_index_distances(const pgb_index* ix, const void* queri
                 rows, ix->n, ix->dim, ix->norm_in_row ? 1u : 0u, (const uint8_t*)queries, nq,
                 query_stride, pairs, npairs, out, bad);
         e = cudaGetLastError();
+        if (e == cudaSuccess) count_launches(1);
     }
     uint32_t hbad = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);

@@ -2,6 +2,7 @@
 // batched; the kernels themselves are in search_flat_kernels.cuh, compiled per adjacency
 // chunk count by search_flat_ch*.cu).
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "errors.h"
@@ -36,6 +37,12 @@ void* pick(int ch, FlatSchedule sched, bool is_signed, uint32_t filter_words) {
 }
 
 }  // namespace
+
+namespace {
+std::atomic<int64_t> g_search_launches{0};
+}  // namespace
+
+void count_launches(int64_t n) { g_search_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int flat_chunks_for(uint32_t gs) {
     int ch = (int)((gs + 31) / 32);
@@ -148,10 +155,15 @@ pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream, const
     }
     if (e != cudaSuccess)
         return fail(PGB_ERR_CUDA, std::string("search launch: ") + cudaGetErrorString(e));
+    count_launches(1);
     return PGB_OK;
 }
 
 }  // namespace pgb
+
+extern "C" uint64_t pgb_search_launches(void) {
+    return (uint64_t)pgb::g_search_launches.load(std::memory_order_relaxed);
+}
 
 extern "C" pgb_status pgb_section_profile(uint64_t* out, uint32_t n, int reset) {
 #ifdef PGB_SECTION_PROFILE

@@ -820,6 +820,7 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
     void* args[] = {&A};
     cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
                                      H.smem_bytes, stream);
+    if (e == cudaSuccess) count_launches(1);
     return hnsw_cuda(e, "HNSW launch");
 }
 

@@ -49,4 +49,8 @@ pgb_status plan_flat(const FlatPlanRequest& rq, FlatPlan& P);
 pgb_status launch_flat(const FlatPlan& P, FlatArgs A, cudaStream_t stream,
                        const pgb_index* ix = nullptr);
 
+// process-wide count of search kernels launched (pgb_search_launches); a negative n takes
+// back launches that were only captured into a graph
+void count_launches(int64_t n);
+
 }  // namespace pgb

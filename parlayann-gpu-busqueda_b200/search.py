@@ -313,6 +313,12 @@ def device_available() -> bool:
     return bool(N.lib.pgb_device_available())
 
 
+def search_launches() -> int:
+    """Search kernels this process has launched through the library (graph replays count
+    their kernels)."""
+    return int(N.lib.pgb_search_launches())
+
+
 class Batch:
     """Batched persistent form: one launch over queries with per-query (Ls, k).
 

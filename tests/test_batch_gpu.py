@@ -212,3 +212,32 @@ def test_batch_host_path_pinned_buffers(pgb, golden, gpu, kind):
         assert_same("stats", st.numpy()[:, :3], s0[:, :3])
     b.close()
     index.close()
+
+
+def test_search_launch_counter(pgb, golden, gpu):
+    """pgb_search_launches counts one launch per search call and per graph replay; the
+    launch recorded while capturing a graph is not a launch."""
+    import torch
+    base, queries = golden.vectors_for("vamana")
+    index = pgb.Index.flat(base, golden.graphs["vamana"])
+    nq = len(queries)
+    q = torch.from_numpy(queries.view(np.uint8)).cuda()
+    s = pgb.Searcher(index, nq, pgb.QueryParams(k=10, beam_size=20))
+    c0 = pgb.search_launches()
+    for _ in range(3):
+        s.search_device(q)
+    assert pgb.search_launches() - c0 == 3
+    b = pgb.Batch(index, nq, max_beam=20, max_k=10)
+    b.plan(np.full(nq, 20), np.full(nq, 10))
+    ids, dists, stats = b.outputs(q.device)
+    c1 = pgb.search_launches()
+    b.search(q, ids, dists, stats)
+    b.capture(q, ids, dists, stats)
+    assert pgb.search_launches() - c1 == 1
+    for _ in range(4):
+        b.replay()
+    torch.cuda.synchronize()
+    assert pgb.search_launches() - c1 == 5
+    b.close()
+    s.liberar()
+    index.close()
