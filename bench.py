@@ -522,6 +522,70 @@ def run_extras(args, pgb, torch, dev, local, base, queries, graph, gt_ids, gt_d,
     return {"identical_to_oracle": ident, "families": families, "serving": serving}
 
 
+def gather_rate(pgb, torch, dev, index, query_dev, lanes, count, steps, warmup, flush,
+                seed=0, sequential=False):
+    """Row-gather rate of pgb_gather_probe: `count` rows (uniformly random ids, or 0..count-1
+    in order) per step, L2 flushed before each step; returns (GB/s of 128-byte rows, the
+    output of the last step)."""
+    n = int(index.info.n_points)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    ids = (torch.arange(count, device=dev, dtype=torch.int64) % n if sequential else
+           torch.randint(0, n, (count,), device=dev, generator=g)).to(torch.int32)
+    out = torch.empty(count, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    t = _timed_events(torch, stream,
+                      lambda: index.gather_probe(query_dev, ids, lanes, out, stream.cuda_stream),
+                      steps, warmup, flush)
+    return count * 128 / (sum(t) / len(t) / 1e3) / 1e9, out
+
+
+def run_gather(args, local):
+    """Gather calibration: the rate at which this B200 gathers random 128-byte rows with
+    1, 4 (the search kernels' layout), 8 and 32 threads per row, from the 1M int8 d=100
+    base (128 MB, about the size of L2) and from a 10M-row table (1.28 GB, HBM), L2
+    flushed before every step; rows read in order give the streaming rate beside it. All
+    layouts compute the same distances (checked)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    from parlayann_gpu_busqueda_b200.formats import Graph
+    base = load_base(pgb)
+    big = np.random.default_rng(5).integers(-128, 128, size=(10_000_000, 100), dtype=np.int8)
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+    count = int(os.environ.get("PGB_GATHER_ROWS", str(20_000_000)))
+    query = torch.from_numpy(rank_queries(0, 1).view(np.uint8)[0].copy()).to(dev)
+    tables = {}
+    peak, kind = measured_peaks()
+    for name, x in (("1M rows (128 MB)", base), ("10M rows (1.28 GB)", big)):
+        n = x.shape[0]
+        chain = Graph(n, 1, np.ones(n, np.uint32), ((np.arange(n) + 1) % n).astype(np.uint32))
+        index = pgb.Index.flat(x, chain, device=local)
+        rows, ref = {}, None
+        for lanes in (4, 1, 8, 32):
+            gbs, out = gather_rate(pgb, torch, dev, index, query, lanes, count, args.steps,
+                                   args.warmup, flush)
+            if ref is None:
+                ref = out.clone()
+            rows[f"{lanes} lanes/row"] = {"gbs": gbs, "frac_of_hbm_peak": gbs / peak,
+                                          "same_distances": bool(torch.equal(out, ref))}
+            log(name, lanes, rows[f"{lanes} lanes/row"])
+        seq, _ = gather_rate(pgb, torch, dev, index, query, 4, min(count, n), args.steps,
+                             args.warmup, flush, sequential=True)
+        rows["rows in order, 4 lanes/row"] = {"gbs": seq, "frac_of_hbm_peak": seq / peak}
+        tables[name] = rows
+        index.close()
+    best = max(r["gbs"] for r in tables["10M rows (1.28 GB)"].values())
+    print(json.dumps({
+        "metric": "random 128-byte row gather rate, 1 B200", "value": best, "unit": "GB/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "dtype": "int8", "data": "synthetic",
+        "config": {"workload": f"{count} rows per step, ids uniform at random; L2 flushed",
+                   "tables": tables, "hbm_peak_gbs": peak, "peak_source": kind},
+        "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -543,7 +607,7 @@ def main():
                     help="warps per block of the profiled batched launch")
     ap.add_argument("--workload", default="vamana",
                     choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "mixed_hnsw", "serving",
-                             "serving_hnsw", "c4", "build", "codes"],
+                             "serving_hnsw", "c4", "build", "codes", "gather"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
                          "mixed / mixed_hnsw: 100k queries of uneven Ls and k in one launch "
@@ -565,11 +629,11 @@ def main():
             run_profile(args, local)
         return
     if args.workload in ("hnsw", "mixed", "mixed_hnsw", "serving", "serving_hnsw", "c4",
-                         "build", "codes") and args.impl == "ours":
+                         "build", "codes", "gather") and args.impl == "ours":
         {"hnsw": run_hnsw, "mixed": run_mixed, "mixed_hnsw": lambda a, lo: run_mixed(a, lo, "hnsw"),
          "serving": run_serving,
          "serving_hnsw": lambda a, lo: run_serving(a, lo, "hnsw"), "c4": run_c4,
-         "build": run_build, "codes": run_codes}[args.workload](args, local)
+         "build": run_build, "codes": run_codes, "gather": run_gather}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -711,6 +775,8 @@ def main():
     avg_plain_s = (sum(t_plain) / len(t_plain)) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = bytes_launch / avg_batch_s / 1e9
+    # empirical ceiling: random rows of this base gathered by the search's row code alone
+    ceiling, _ = gather_rate(pgb, torch, dev, index, q_dev[0], 4, 20_000_000, 5, 2, flush)
     traffic = None
     tp = os.path.join(ROOT, "profiles", "flat_batched_c2_traffic.json")
     if os.path.exists(tp):
@@ -787,6 +853,8 @@ def main():
                          "kernel": "flat_batched_kernel", "bytes_per_launch": bytes_launch,
                          "avg_launch_ms": avg_batch_s * 1e3,
                          "plain_frac": bytes_launch / avg_plain_s / 1e9 / peak,
+                         "gather_ceiling_gbs": ceiling,
+                         "frac_of_gather_ceiling": achieved / ceiling,
                          "comps_per_query": float(st[:, 0].mean()),
                          "expansions_per_query": float(st[:, 1].mean())},
             "cpu_baseline": cpu_baseline,

@@ -146,6 +146,14 @@ pgb_status pgb_index_distances(const pgb_index* index, const void* queries, uint
                                uint32_t query_stride, const uint32_t* pairs, uint64_t npairs,
                                int32_t* out, void* stream);
 
+/* Gather calibration: the int32 squared L2 distance of one query (device, index dim bytes)
+ * to count rows named by ids (device) into out, computed with lanes_per_row threads per
+ * 128-byte row (1, 4, 8 or 32). Asynchronous on `stream`. It measures the device's random
+ * row-gather rate, as the reference's micro_distancias.cu:19-63 does for its kernels;
+ * lanes_per_row 4 is the search kernels' own row code. Ids >= n get INT32_MIN. */
+pgb_status pgb_gather_probe(const pgb_index* index, const void* query, const uint32_t* ids,
+                            uint64_t count, int32_t* out, uint32_t lanes_per_row, void* stream);
+
 /* L2 residency (no counterpart in the reference): an access-policy window over one region
  * of a flat index -- PGB_L2_ROWS (the 128-byte vector rows), PGB_L2_CODES (the 64-byte
  * code rows of pgb_index_compress) or PGB_L2_GRAPH (the adjacency rows) -- carried by every

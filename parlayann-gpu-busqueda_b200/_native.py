@@ -83,6 +83,7 @@ _sig("pgb_searcher_search_host", C.c_int, vp, vp, u32, u32, vp, vp, vp)
 _sig("pgb_searcher_destroy", C.c_int, vp)
 _sig("pgb_index_compress", C.c_int, vp, i32, vp)
 _sig("pgb_search_launches", u64)
+_sig("pgb_gather_probe", C.c_int, vp, vp, vp, u64, vp, u32, vp)
 _sig("pgb_index_distances", C.c_int, vp, vp, u32, u32, vp, u64, vp, vp)
 _sig("pgb_index_set_l2_window", C.c_int, vp, u32, u64, C.POINTER(u64), C.POINTER(C.c_float))
 L2_NONE, L2_ROWS, L2_CODES, L2_GRAPH = 0, 1, 2, 3

@@ -122,3 +122,154 @@ extern "C" pgb_status pgb_index_distances(const pgb_index* ix, const void* queri
     if (hbad) return fail(PGB_ERR_BAD_ARG, "a pair names a query or point out of range (its output is INT32_MIN)");
     return PGB_OK;
 }
+
+// ---- gather calibration ----------------------------------------------------------------
+// pgb_gather_probe: the distance of one query to n rows named by ids, with LANES threads
+// per 128-byte row, to measure how fast this device gathers random rows (the reference
+// measures the same, cuda/micro_distancias.cu:19-63). LANES 4 runs the search kernels' own
+// row code (row_round, two slots: 16 rows in flight per warp, each load instruction
+// covering whole 32-byte sectors of 8 rows); 1, 8 and 32 are the alternatives it was
+// chosen over. Ids >= n give INT32_MIN (the row read is row 0's).
+namespace pgb {
+namespace {
+
+constexpr int kProbeWarps = 4;
+
+template <bool Signed, int LANES>
+__global__ void __launch_bounds__(kProbeWarps * 32) gather_probe_kernel(
+    const uint8_t* __restrict__ rows, uint32_t n, uint32_t dim, uint32_t norm_in_row,
+    const uint8_t* __restrict__ query, const uint32_t* __restrict__ ids, uint64_t count,
+    int32_t* __restrict__ out) {
+    __shared__ __align__(16) uint32_t qrow[32];
+    __shared__ uint32_t sid[kProbeWarps][16];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x < 32) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const uint32_t i = 4u * threadIdx.x + b;
+            v |= (uint32_t)(i < dim ? query[i] : 0u) << (8 * b);
+        }
+        qrow[threadIdx.x] = v;
+    }
+    __syncthreads();
+    const int4* q4 = reinterpret_cast<const int4*>(qrow);
+    const bool nir = norm_in_row != 0;
+    const uint64_t warp = (uint64_t)blockIdx.x * kProbeWarps + w;
+    const uint64_t warps = (uint64_t)gridDim.x * kProbeWarps;
+    if constexpr (LANES == 4) {
+        // the search's layout: 16 rows per warp per round, ids staged in shared memory
+        const int grp = lane >> 2, c = lane & 3;
+        const int4 qa = q4[c], qb = q4[c + 4];
+        int32_t qq = partial_sq<Signed>(qa) + partial_sq<Signed>(qb);
+        qq += __shfl_xor_sync(kFull, qq, 2, 4);
+        qq += __shfl_xor_sync(kFull, qq, 1, 4);
+        const bool need_a = (uint32_t)(c * 16) < dim;
+        const bool need_b = (uint32_t)((c + 4) * 16) < dim || (nir && c == 3);
+        for (uint64_t base = warp * 16u; base < count; base += warps * 16u) {
+            const int np = count - base < 16u ? (int)(count - base) : 16;
+            if (lane < np) {
+                const uint32_t id = __ldg(ids + base + lane);
+                sid[w][lane] = id < n ? id : 0u;
+            }
+            __syncwarp();
+            row_round<Signed, 2>(rows, sid[w], out + base, np, 0, qa, qb, qq, need_a, need_b, nir, grp, c);
+            __syncwarp();
+            if (lane < np && __ldg(ids + base + lane) >= n) out[base + lane] = INT32_MIN;
+            __syncwarp();
+        }
+    } else {
+        // LANES threads per row, each reading 128 / LANES bytes; rows per warp per round:
+        // 32 / LANES, times SLOTS rows in flight per group
+        constexpr int GROUPS = 32 / LANES;
+        constexpr int SLOTS = LANES == 1 ? 1 : (LANES == 8 ? 2 : 4);
+        constexpr int BYTES = 128 / LANES;
+        const int grp = lane / LANES, c = lane % LANES;
+        int32_t qq = partial_sq<Signed>(q4[lane & 7]);
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) qq += __shfl_xor_sync(kFull, qq, off, 8);
+        for (uint64_t base = warp * (GROUPS * SLOTS); base < count; base += warps * (GROUPS * SLOTS)) {
+            int32_t t[SLOTS];
+            uint32_t rid[SLOTS];
+#pragma unroll
+            for (int r = 0; r < SLOTS; r++) {
+                const uint64_t i = base + (uint64_t)r * GROUPS + grp;
+                const uint32_t id = i < count ? __ldg(ids + i) : 0u;
+                rid[r] = id;
+                const uint8_t* row = rows + (size_t)(id < n ? id : 0u) * kRowBytes + c * BYTES;
+                int32_t acc = 0;
+                if constexpr (BYTES >= 16) {
+#pragma unroll
+                    for (int j = 0; j < BYTES / 16; j++) {
+                        const int wd = c * (BYTES / 16) + j;  // 16-byte word of the row
+                        const int4 v = ldg16(row + 16 * j);
+                        acc += (nir ? (wd == 7 ? v.w : 0) - 2 * partial_dot<Signed>(v, q4[wd])
+                                    : partial_l2<Signed>(v, q4[wd]));
+                    }
+                } else {
+                    const int32_t v = __ldg(reinterpret_cast<const int32_t*>(row));
+                    const int32_t qw = (int32_t)qrow[c];
+                    int32_t d;
+                    if (Signed) d = __dp4a(v, qw, 0);
+                    else d = (int32_t)__dp4a((uint32_t)v, (uint32_t)qw, 0u);
+                    int32_t pp;
+                    if (Signed) pp = __dp4a(v, v, 0);
+                    else pp = (int32_t)__dp4a((uint32_t)v, (uint32_t)v, 0u);
+                    acc = nir ? (c == 31 ? v : 0) - 2 * d : pp - 2 * d;
+                }
+                t[r] = acc;
+            }
+#pragma unroll
+            for (int off = LANES / 2; off > 0; off >>= 1)
+#pragma unroll
+                for (int r = 0; r < SLOTS; r++) t[r] += __shfl_xor_sync(kFull, t[r], off, LANES);
+            if (c == 0) {
+#pragma unroll
+                for (int r = 0; r < SLOTS; r++) {
+                    const uint64_t i = base + (uint64_t)r * GROUPS + grp;
+                    if (i < count) out[i] = rid[r] < n ? qq + t[r] : INT32_MIN;
+                }
+            }
+        }
+    }
+}
+
+template <int LANES>
+void* probe_kernel(bool is_signed) {
+    return is_signed ? (void*)gather_probe_kernel<true, LANES> : (void*)gather_probe_kernel<false, LANES>;
+}
+
+}  // namespace
+}  // namespace pgb
+
+extern "C" pgb_status pgb_gather_probe(const pgb_index* ix, const void* query, const uint32_t* ids,
+                                       uint64_t count, int32_t* out, uint32_t lanes_per_row,
+                                       void* stream) {
+    if (!ix) return fail(PGB_ERR_BAD_ARG, "null index");
+    if (count == 0) return PGB_OK;
+    if (!query || !ids || !out) return fail(PGB_ERR_BAD_ARG, "null query, ids or output");
+    void* kern = nullptr;
+    const bool sg = ix->elem == PGB_INT8;
+    switch (lanes_per_row) {
+        case 1: kern = probe_kernel<1>(sg); break;
+        case 4: kern = probe_kernel<4>(sg); break;
+        case 8: kern = probe_kernel<8>(sg); break;
+        case 32: kern = probe_kernel<32>(sg); break;
+        default: return fail(PGB_ERR_BAD_ARG, "lanes_per_row must be 1, 4, 8 or 32");
+    }
+    DeviceGuard guard(ix->device);
+    if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
+    int dev = 0, sms = 148, per_sm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kProbeWarps * 32, 0) != cudaSuccess || per_sm < 1)
+        per_sm = 1;
+    const uint8_t* rows = ix->rows;
+    uint32_t n = ix->n, dim = ix->dim, nir = ix->norm_in_row ? 1u : 0u;
+    const uint8_t* q = (const uint8_t*)query;
+    void* args[] = {&rows, &n, &dim, &nir, &q, &ids, &count, &out};
+    const cudaError_t e = cudaLaunchKernel(kern, dim3((unsigned)(sms * per_sm)), dim3(kProbeWarps * 32),
+                                           args, 0, (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_status(e, "gather probe");
+    count_launches(1);
+    return PGB_OK;
+}

@@ -134,6 +134,16 @@ class Index:
                                           npairs, _ptr(out), C.c_void_p(stream)))
         return out[:npairs].cpu().numpy()
 
+    def gather_probe(self, query, ids, lanes_per_row: int, out=None, stream: int = 0):
+        """Distances of one device query row to the rows `ids` (CUDA uint32 tensor) with
+        lanes_per_row threads per row; returns the output tensor (asynchronous)."""
+        import torch
+        if out is None:
+            out = torch.empty(ids.shape[0], dtype=torch.int32, device=ids.device)
+        N.check(N.lib.pgb_gather_probe(self._h, _ptr(query), _ptr(ids), ids.shape[0], _ptr(out),
+                                       lanes_per_row, C.c_void_p(stream)))
+        return out
+
     def codes(self, rows: bool = True):
         """(step, offsets int32 [dim], code rows uint8 [n, 64] or None)."""
         step = C.c_int32()

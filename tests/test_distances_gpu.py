@@ -70,3 +70,29 @@ def test_pair_distances_reject_out_of_range(pgb, gpu):
     with pytest.raises(pgb.PgbError, match="out of range"):
         index.distances(base[:2], np.array([[2, 3]], np.uint32))
     index.close()
+
+
+@pytest.mark.parametrize("dtype,dim", [(np.int8, 100), (np.uint8, 128), (np.int8, 33)])
+def test_gather_probe_layouts_agree(pgb, oracle, gpu, dtype, dim):
+    """The gather calibration's four layouts (1, 4, 8 and 32 threads per row) compute the
+    exact distances of the pair-distance entry point; ids past the table give INT32_MIN."""
+    import torch
+    rng = np.random.default_rng(2)
+    info = np.iinfo(dtype)
+    n = 5_000
+    base = rng.integers(info.min, int(info.max) + 1, size=(n, dim)).astype(dtype)
+    query = rng.integers(info.min, int(info.max) + 1, size=(1, dim)).astype(dtype)
+    index = pgb.Index.flat(base, chain_graph(n))
+    ids = rng.integers(0, n, 20_011).astype(np.uint32)
+    ids[::997] = n + 7  # out of range
+    want = oracle.pair_distances(base, query, np.stack([np.zeros_like(ids), np.minimum(ids, n - 1)], 1))
+    want = np.where(ids >= n, np.iinfo(np.int32).min, want)
+    q = torch.from_numpy(query.view(np.uint8)[0].copy()).cuda()
+    tid = torch.from_numpy(ids.view(np.int32)).cuda()
+    for lanes in (1, 4, 8, 32):
+        got = index.gather_probe(q, tid, lanes)
+        torch.cuda.synchronize()
+        assert_same(f"{lanes} lanes/row", got.cpu().numpy(), want)
+    with pytest.raises(pgb.PgbError, match="lanes_per_row"):
+        index.gather_probe(q, tid, 2)
+    index.close()
