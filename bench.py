@@ -1217,9 +1217,9 @@ def run_c4(args, local):
 
 def run_mixed(args, local, kind="vamana"):
     """100,000 queries with Ls log-uniform in [10, 500] and k in {10, 50, 100}: one batched
-    launch (a CUDA graph on the Vamana graph) against the plain kernel launched once per
-    distinct (Ls, k); kind "hnsw": the same on the HNSW model (the batched launch is not
-    captured: beams above 256 use the epoch-tagged filter)."""
+    launch (a CUDA graph) against the plain kernel launched once per distinct (Ls, k);
+    kind "hnsw": the same on the HNSW model (its beams above 256 use the (epoch, id) filter,
+    whose epochs come from a device word, so the graph replays with fresh ones)."""
     import torch
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -1246,11 +1246,8 @@ def run_mixed(args, local, kind="vamana"):
     tuned = b.tune(q, ids, d, st)
     flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
     steps = max(3, args.steps // 20)
-    if kind == "hnsw":
-        tb = _timed_events(torch, stream, lambda: b.search(q, ids, d, st, sp), steps, 2, flush)
-    else:
-        b.capture(q, ids, d, st)
-        tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, 2, flush)
+    b.capture(q, ids, d, st)
+    tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, 2, flush)
     # plain: the drop-in prepares one searcher per distinct (Ls, k) and launches it on
     # that group's queries; preparing and releasing are outside the timed launches
     groups = {}

@@ -247,7 +247,7 @@ pgb_status pgb_search_flat_noalloc(const pgb_index* index, const pgb_query_param
  * a block. Neighbours are identical to pgb_searcher_search with the same per-query params.
  * Outputs use a row stride of max_k; row q holds k_q entries then padding. On an HNSW
  * index the launch runs the HNSW kernel (cut, degree_limit, exclude_query_id and the
- * placement options do not apply; graph capture needs max_beam <= 256). */
+ * placement options do not apply). */
 typedef struct pgb_batch_options {
     uint32_t max_queries;
     uint32_t max_beam;          /* largest Ls planned                                   */

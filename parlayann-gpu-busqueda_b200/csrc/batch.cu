@@ -7,7 +7,8 @@
 //          queries and keeps the fastest; every candidate returns identical neighbours,
 //          because all of them run the same per-query code (flat_query)
 // An HNSW index runs the HNSW kernel with each query at its own (Ls, k), its tables sized
-// for max_beam; it has a single launch shape, so tune only times it.
+// for max_beam; it has a single launch shape, so tune only times it. Every beam can be
+// captured: the (epoch, id) filter of beams above 256 takes its epochs from a device word.
 #include <algorithm>
 #include <numeric>
 #include <string>
@@ -40,6 +41,7 @@ struct pgb_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int64_t graph_launches = 0;  // search kernels in the captured graph
+    uint64_t graph_epochs = 0;   // HNSW (epoch, id) filter: epochs one replay uses
     // host-memory path staging
     uint8_t* q_dev = nullptr;
     uint32_t* ids_dev = nullptr;
@@ -387,10 +389,6 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
                              int32_t* dists, pgb_query_stats* stats) {
     pgb_status s = check_call(b, queries, qstride, ids, dists);
     if (s != PGB_OK) return s;
-    // HNSW beams above 256 use a global (epoch, id) filter whose epochs advance on every
-    // launch; a replayed graph would repeat them and see the last replay's entries
-    if (b->hnsw && b->hs.fmode == 2)
-        return fail(PGB_ERR_BAD_ARG, "graph capture on HNSW needs max_beam <= 256");
     DeviceGuard guard(b->index->device);
     if (!guard.ok) return fail(PGB_ERR_CUDA, "cudaSetDevice failed");
     drop_graph(b);
@@ -402,9 +400,15 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
         // launches made during the capture only record graph nodes: they count once per
         // replay instead
         const int64_t before = (int64_t)pgb_search_launches();
+        // an HNSW (epoch, id) filter (beams above 256): the captured launch reads its first
+        // epoch from the device word that the graph's last node advances, so every replay
+        // searches with fresh epochs; the host mirror is reserved per replay instead
+        const uint64_t epochs_before = b->hs.epoch_base;
         pgb_status ls = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
         b->graph_launches = (int64_t)pgb_search_launches() - before;
         count_launches(-b->graph_launches);
+        b->graph_epochs = (b->hnsw && b->hs.d_epoch) ? hnsw_epoch_need(b->index, b->nq) : 0;
+        b->hs.epoch_base = epochs_before;
         cudaGraph_t g = nullptr;
         e = cudaStreamEndCapture(st, &g);
         if (ls != PGB_OK) {
@@ -429,6 +433,10 @@ pgb_status pgb_batch_capture(pgb_batch* b, const void* queries, uint32_t qstride
 pgb_status pgb_batch_replay(pgb_batch* b, void* stream) {
     if (!b || !b->graph_exec) return fail(PGB_ERR_BAD_ARG, "no captured graph");
     DeviceGuard guard(b->index->device);
+    if (b->graph_epochs) {
+        const pgb_status r = hnsw_epoch_reserve(b->hs, b->graph_epochs, (cudaStream_t)stream);
+        if (r != PGB_OK) return r;
+    }
     const pgb_status s = cuda_status(cudaGraphLaunch(b->graph_exec, (cudaStream_t)stream), "graph launch");
     if (s == PGB_OK) count_launches(b->graph_launches);
     return s;

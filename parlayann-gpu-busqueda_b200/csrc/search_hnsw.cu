@@ -113,6 +113,10 @@ struct HnswArgs {
     pgb_query_stats* stats;
     unsigned long long* gfilter;
     uint64_t epoch_base;
+    // (epoch, id) filter: the launch's first epoch read from device memory (a captured
+    // graph replays one launch; hnsw_epoch_advance moves this word on after each launch);
+    // null: epoch_base
+    const uint64_t* epoch_ptr;
     uint32_t* queue;  // query work queue: each warp takes the next query when it is free
     uint32_t out_stride;  // query q's k outputs start at q * out_stride
     // batched launch (else null): query q's beam and k, and the order the queue hands the
@@ -190,6 +194,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
     const int ccap = (int)hnsw_ccap(L.wcap);
     const uint32_t lt = lanemask_lt(), gt = lanemask_gt();
     const uint32_t layers = A.top + 1u;
+    const uint64_t epoch_base = (FMODE == 2 && A.epoch_ptr) ? *A.epoch_ptr : A.epoch_base;
     // queries are taken from the work queue, so a warp that drew short searches takes more
     // of them and the launch does not wait on the warps with the longest share
     auto take = [&]() -> uint32_t {
@@ -236,7 +241,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             const uint32_t stride = (layer > 0) ? A.gas : A.g0s;
             const int G = (int)((layer > 0) ? A.GA : A.G0);
             const uint32_t epoch =
-                (uint32_t)(A.epoch_base + (uint64_t)q * layers + (A.top - (uint32_t)layer) + 1u);
+                (uint32_t)(epoch_base + (uint64_t)q * layers + (A.top - (uint32_t)layer) + 1u);
             if (SFILT) {
                 for (uint32_t i = lane; i <= fmask; i += 32) sfilter[i] = kEmptyId;
             } else if (FMODE == 1) {
@@ -736,12 +741,18 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
         const size_t fb = 8ull * H.filter_slots * H.total_warps;
         if ((s = hnsw_cuda(cudaMalloc(&H.gfilter, fb), "filter tables")) != PGB_OK) return s;
         if ((s = hnsw_cuda(cudaMemset(H.gfilter, 0, fb), "filter clear")) != PGB_OK) return s;
+        if ((s = hnsw_cuda(cudaMalloc(&H.d_epoch, sizeof(uint64_t)), "epoch word")) != PGB_OK) return s;
+        if ((s = hnsw_cuda(cudaMemset(H.d_epoch, 0, sizeof(uint64_t)), "epoch word")) != PGB_OK) return s;
     }
     H.epoch_base = 0;
     H.max_ls = Ls;
     H.ready = true;
     return PGB_OK;
 }
+
+// moves the device epoch word past the epochs the launch before it used (stream order:
+// the search kernel has finished reading it)
+__global__ void hnsw_epoch_advance(uint64_t* epoch, uint64_t need) { *epoch += need; }
 
 pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params& p,
                        const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
@@ -800,18 +811,15 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
     A.stats = stats;
     A.gfilter = H.gfilter;
     // every (query, layer) of every launch gets a fresh epoch for an (epoch, id) global
-    // filter; wrap -> clear it
-    const uint64_t need = (uint64_t)nq * (ix->top_level + 1ull) + 1ull;
-    if (H.epoch_base + need >= 0xFFFFFFFFull) {
-        pgb_status s;
-        if (H.fmode == 2 &&
-            (s = hnsw_cuda(cudaMemsetAsync(H.gfilter, 0, 8ull * H.filter_slots * H.total_warps, stream),
-                           "filter clear")) != PGB_OK)
-            return s;
-        H.epoch_base = 0;
+    // filter; the device word d_epoch holds the next unused one and H.epoch_base mirrors it
+    // on the host (hnsw_epoch_reserve; wrap -> clear the tables)
+    const uint64_t need = hnsw_epoch_need(ix, nq);
+    {
+        const pgb_status s = hnsw_epoch_reserve(H, need, stream);
+        if (s != PGB_OK) return s;
     }
-    A.epoch_base = H.epoch_base;
-    H.epoch_base += need;
+    A.epoch_base = H.epoch_base - need;
+    A.epoch_ptr = H.d_epoch;
     A.queue = H.queue;
     {
         const pgb_status s = hnsw_cuda(cudaMemsetAsync(H.queue, 0, sizeof(uint32_t), stream), "query queue");
@@ -821,7 +829,29 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
     cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
                                      H.smem_bytes, stream);
     if (e == cudaSuccess) count_launches(1);
+    if (e == cudaSuccess && H.d_epoch) {
+        hnsw_epoch_advance<<<1, 1, 0, stream>>>(H.d_epoch, need);
+        e = cudaGetLastError();
+    }
     return hnsw_cuda(e, "HNSW launch");
+}
+
+uint64_t hnsw_epoch_need(const pgb_index* ix, uint32_t nq) {
+    return (uint64_t)nq * (ix->top_level + 1ull) + 1ull;
+}
+
+pgb_status hnsw_epoch_reserve(HnswState& H, uint64_t need, cudaStream_t stream) {
+    if (H.epoch_base + need >= 0xFFFFFFFFull) {
+        pgb_status s;
+        if (H.fmode == 2 &&
+            ((s = hnsw_cuda(cudaMemsetAsync(H.gfilter, 0, 8ull * H.filter_slots * H.total_warps, stream),
+                            "filter clear")) != PGB_OK ||
+             (s = hnsw_cuda(cudaMemsetAsync(H.d_epoch, 0, sizeof(uint64_t), stream), "epoch reset")) != PGB_OK))
+            return s;
+        H.epoch_base = 0;
+    }
+    H.epoch_base += need;
+    return PGB_OK;
 }
 
 cudaError_t hnsw_section_totals(unsigned long long* acc, bool reset) {
@@ -845,6 +875,7 @@ cudaError_t hnsw_section_totals(unsigned long long* acc, bool reset) {
 void hnsw_release(HnswState& H) {
     cudaFree(H.gfilter);
     cudaFree(H.queue);
+    cudaFree(H.d_epoch);
     H = HnswState{};
 }
 

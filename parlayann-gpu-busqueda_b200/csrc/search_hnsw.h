@@ -27,6 +27,9 @@ struct HnswState {
     unsigned long long* gfilter = nullptr; // global lossy filter per warp: 4-byte ids
                                            // (fmode 1) or (epoch, id) pairs (fmode 2)
     uint64_t epoch_base = 0;               // next unused epoch (tables start at epoch 0)
+    uint64_t* d_epoch = nullptr;           // fmode 2: the same on the device, read by each
+                                           // launch and advanced after it (captured
+                                           // graphs replay with fresh epochs)
     uint32_t max_ls = 0;                   // the beam the state was prepared for
     uint32_t* queue = nullptr;             // next query of the running launch (zeroed per launch)
 };
@@ -44,6 +47,10 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
                           int32_t* dists, pgb_query_stats* stats, uint32_t out_stride,
                           cudaStream_t stream, const uint32_t* ls_arr = nullptr,
                           const uint32_t* k_arr = nullptr, const uint32_t* order = nullptr);
+// epochs one launch of nq queries uses, and their reservation on the host mirror of the
+// device epoch word (a wrap enqueues a clear of the tables and of the word on `stream`)
+uint64_t hnsw_epoch_need(const pgb_index* ix, uint32_t nq);
+pgb_status hnsw_epoch_reserve(HnswState& H, uint64_t need, cudaStream_t stream);
 // device bytes of the state's scratch tables
 size_t hnsw_scratch_bytes(const HnswState& H);
 void hnsw_release(HnswState& H);

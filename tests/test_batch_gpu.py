@@ -141,7 +141,8 @@ def test_batch_hnsw_mixed_beams_match_oracle(pgb, oracle, golden, gpu, max_beam)
     """HNSW in the batched form: each query at its own (Ls, k) in one launch of the HNSW
     kernel, tables sized for max_beam (300: the (epoch, id) global filter); the answer of
     every query, its distance count and its flags are the oracle's for its (Ls, k). A
-    captured graph replays to the same answer (beams up to 256 only)."""
+    captured graph replays to the same answer, each replay with fresh filter epochs, also
+    between direct launches of the same batch."""
     import torch
     base, queries = golden.vectors_for("hnsw")
     h = golden.hnsw["hnsw"]
@@ -167,18 +168,20 @@ def test_batch_hnsw_mixed_beams_match_oracle(pgb, oracle, golden, gpu, max_beam)
         assert_same(f"q{qi} comps/exps/flags", st[qi, :3], [oc[0], oe[0], of[0]])
     cfg = b.tune(q, ids, dists, stats)
     assert cfg["tuned_ms"] > 0
-    if max_beam <= 256:
-        b.capture(q, ids, dists, stats)
-        for _ in range(2):
-            ids.fill_(0)
+    b.capture(q, ids, dists, stats)
+    for r in range(4):
+        ids.fill_(0)
+        dists.fill_(0)
+        if r == 2:
+            b.search(q, ids, dists, stats)  # a direct launch between replays
+        else:
             b.replay()
-            torch.cuda.synchronize()
-            rep = ids.cpu().numpy().view(np.uint32)
-            for qi in range(nq):
-                assert_same(f"replay q{qi}", rep[qi, :ks[qi]], got_i[qi, :ks[qi]])
-    else:
-        with pytest.raises(pgb.PgbError, match="256"):
-            b.capture(q, ids, dists, stats)
+        torch.cuda.synchronize()
+        rep_i = ids.cpu().numpy().view(np.uint32)
+        rep_d = dists.cpu().numpy()
+        for qi in range(nq):
+            assert_same(f"replay {r} q{qi} ids", rep_i[qi, :ks[qi]], got_i[qi, :ks[qi]])
+            assert_same(f"replay {r} q{qi} dists", rep_d[qi, :ks[qi]], got_d[qi, :ks[qi]])
     b.close()
     index.close()
 
