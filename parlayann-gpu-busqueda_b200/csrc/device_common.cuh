@@ -151,6 +151,14 @@ __device__ __forceinline__ int32_t partial_sq(const int4 q) {
     }
 }
 
+// Marks one query of a launch as finished for a host observer: every lane's output writes
+// are made visible at system scope before lane 0 stores the flag (host-mapped memory).
+__device__ __forceinline__ void publish_query_done(uint32_t* done, uint32_t q, uint32_t seq, int lane) {
+    __threadfence_system();
+    __syncwarp();
+    if (lane == 0) *reinterpret_cast<volatile uint32_t*>(done + q) = seq;
+}
+
 // read-only 16-byte load through the non-coherent path
 __device__ __forceinline__ int4 ldg16(const void* p) {
     return __ldg(reinterpret_cast<const int4*>(p));

@@ -180,6 +180,11 @@ struct FlatArgs {
     uint32_t* gvisited;             // per-warp global visited tables when not in shared
     uint32_t gvisited_words;
     uint32_t* queue;                // batched: next-query counter
+    // batched, optional: per-query completion flags in host-mapped memory. When query q's
+    // outputs are written (system-visible), done[q] = done_seq, so a host thread can take
+    // the query's results before the launch ends (the serving loop does)
+    uint32_t* done;
+    uint32_t done_seq;
     // code rows (kPlainCodes): rows holds n x 64-byte code rows, a dimension's value is
     // code_step * code + its offset (code_off: one 128-byte row of element values)
     int32_t code_step;

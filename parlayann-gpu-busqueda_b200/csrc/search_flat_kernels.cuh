@@ -84,6 +84,7 @@ __global__ void __launch_bounds__(128, PGB_MIN_BLOCKS) flat_batched_kernel(FlatA
             flat_query<CH, Signed, FW, false, true>(A, wmem, gf, gv, q, A.Ls, A.k, lane);
         else
             flat_query<CH, Signed, FW, false, true>(A, wmem, gf, gv, q, A.ls_arr[q], A.k_arr[q], lane);
+        if (A.done) publish_query_done(A.done, q, A.done_seq, lane);
     }
     PGB_PROF_EXIT();
 }

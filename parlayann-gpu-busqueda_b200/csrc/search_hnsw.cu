@@ -35,6 +35,11 @@
 #include "search_hnsw.h"
 #include "search_plan.h"
 
+// largest lossy filter kept in shared memory (bytes); larger ones live in global memory
+#ifndef PGB_HNSW_SHARED_FILTER_BYTES
+#define PGB_HNSW_SHARED_FILTER_BYTES 4096
+#endif
+
 namespace pgb {
 
 __host__ __device__ inline uint32_t hnsw_bits0(uint32_t Ls) {
@@ -124,6 +129,10 @@ struct HnswArgs {
     const uint32_t* ls_arr;
     const uint32_t* k_arr;
     const uint32_t* order;
+    // optional per-query completion flags in host-mapped memory (done[q] = done_seq once
+    // query q's outputs are system-visible)
+    uint32_t* done;
+    uint32_t done_seq;
 };
 
 __device__ __forceinline__ unsigned long long tag(uint32_t epoch, uint32_t id) {
@@ -638,6 +647,7 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
             A.stats[q] = s;
         }
         __syncwarp();
+        if (A.done) publish_query_done(A.done, q, A.done_seq, lane);
         PGB_PROF_ADD(SEC_SETUP, tp);
     }
 #ifdef PGB_SECTION_PROFILE
@@ -700,7 +710,7 @@ pgb_status hnsw_prepare(const pgb_index* ix, const pgb_query_params& p, HnswStat
     // kernel at 8 resident warps per SM. Up to 16,384 slots (Ls <= 256) the global table
     // holds bare ids beside a written-slot bitmap in shared memory (2 KB at most); larger
     // filters use (epoch, id) pairs.
-    H.fmode = 4ull * fwords <= 4096 ? 0 : (fwords <= 16384 ? 1 : 2);
+    H.fmode = 4ull * fwords <= PGB_HNSW_SHARED_FILTER_BYTES ? 0 : (fwords <= 16384 ? 1 : 2);
     H.filter_slots = H.fmode ? fwords : 0u;
     H.wcap = ((std::max<uint32_t>(Ls, PGB_MAX_HNSW_ENTRIES) + 8u) + 7u) & ~7u;
     const HnswLayout L = hnsw_layout_of(H);
@@ -770,11 +780,13 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
                           const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
                           int32_t* dists, pgb_query_stats* stats, uint32_t out_stride,
                           cudaStream_t stream, const uint32_t* ls_arr, const uint32_t* k_arr,
-                          const uint32_t* order) {
+                          const uint32_t* order, uint32_t* done, uint32_t done_seq) {
     if (!H.ready) return fail(PGB_ERR_BAD_ARG, "HNSW searcher not prepared");
     if (Ls == 0 || Ls > H.max_ls || k == 0 || out_stride < k || (ls_arr == nullptr) != (k_arr == nullptr))
         return fail(PGB_ERR_BAD_ARG, "HNSW launch: beam above the prepared one, or bad k / stride");
     HnswArgs A{};
+    A.done = done;
+    A.done_seq = done_seq;
     A.ls_arr = ls_arr;
     A.k_arr = k_arr;
     A.order = order;
@@ -826,8 +838,44 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
         if (s != PGB_OK) return s;
     }
     void* args[] = {&A};
+#ifdef PGB_HNSW_PERSIST_FILTER
+    cudaError_t e;
+    if (H.fmode == 1) {
+        // experiment: the global filter tables as a persisting L2 window
+        static bool limit_set = false;
+        int dev = 0, maxw = 0, maxp = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev);
+        cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev);
+        const size_t tb = 4ull * H.filter_slots * H.total_warps;
+        const size_t win = std::min<size_t>(tb, (size_t)maxw);
+        if (!limit_set) {
+            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, std::min<size_t>(win, (size_t)maxp));
+            limit_set = true;
+        }
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(H.blocks);
+        cfg.blockDim = dim3(H.warps_per_block * 32);
+        cfg.dynamicSmemBytes = H.smem_bytes;
+        cfg.stream = stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeAccessPolicyWindow;
+        at[0].val.accessPolicyWindow.base_ptr = H.gfilter;
+        at[0].val.accessPolicyWindow.num_bytes = win;
+        at[0].val.accessPolicyWindow.hitRatio = std::min(1.0f, (float)maxp / (float)win);
+        at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelExC(&cfg, H.kernel, args);
+    } else {
+        e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
+                             H.smem_bytes, stream);
+    }
+#else
     cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
                                      H.smem_bytes, stream);
+#endif
     if (e == cudaSuccess) count_launches(1);
     if (e == cudaSuccess && H.d_epoch) {
         hnsw_epoch_advance<<<1, 1, 0, stream>>>(H.d_epoch, need);

@@ -42,11 +42,13 @@ pgb_status hnsw_launch(const pgb_index* ix, HnswState& H, const pgb_query_params
 // filter size and is_inw capacity follow Ls; the tables were sized for H.max_ls). With
 // ls_arr / k_arr (device, every beam <= H.max_ls, every k <= out_stride) query q runs at
 // its own beam and k, and the work queue hands the queries out in `order` (may be null).
+// done (host-mapped, may be null): done[q] = done_seq once query q's outputs are visible.
 pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32_t k, int64_t limit,
                           const void* queries, uint32_t nq, uint32_t qstride, uint32_t* ids,
                           int32_t* dists, pgb_query_stats* stats, uint32_t out_stride,
                           cudaStream_t stream, const uint32_t* ls_arr = nullptr,
-                          const uint32_t* k_arr = nullptr, const uint32_t* order = nullptr);
+                          const uint32_t* k_arr = nullptr, const uint32_t* order = nullptr,
+                          uint32_t* done = nullptr, uint32_t done_seq = 0);
 // epochs one launch of nq queries uses, and their reservation on the host mirror of the
 // device epoch word (a wrap enqueues a clear of the tables and of the word on `stream`)
 uint64_t hnsw_epoch_need(const pgb_index* ix, uint32_t nq);

@@ -5,10 +5,13 @@
 // Host side: submit() admits a request into a bounded slot pool (busy when full) and
 // wakes the dispatcher thread. The dispatcher completes finished launches (event query),
 // then packs the pending requests into batches -- longest beam first -- and launches each
-// on a free stream context: one upload of the packed queries and per-request (Ls, k),
-// one work-queue launch of the batched kernel (the grid shrinks to the batch), one
-// download per output array. New arrivals therefore start while earlier launches are
-// still on the GPU, and their work overlaps on the device. Every request runs the same
+// on a free stream context: one upload of the packed queries and per-request (Ls, k) and
+// one work-queue launch of the batched kernel (the grid shrinks to the batch), which
+// writes each query's outputs into the context's page-locked host buffers and then sets
+// the query's completion flag there. The dispatcher publishes a request as soon as its
+// flag is set, so a short query does not wait for the longest one of its batch; the
+// launch's event frees the context. New arrivals start while earlier launches are still
+// on the GPU, and their work overlaps on the device. Every request runs the same
 // per-query code as the plain searcher, so its answer does not depend on the mix.
 //
 // Locking: one mutex guards the pending queue, the free-slot list, the counters and the
@@ -61,13 +64,19 @@ struct Context {
     bool busy = false;            // written by the dispatcher under the lock
     std::vector<uint32_t> slots;  // pool slots, batch-local order
     uint8_t* h_in = nullptr;      // pinned: queries | ls | k | order
+    // pinned outputs, written by the kernel through their device addresses (d_*), and the
+    // per-query completion flags (h_done[j] == seq: batch position j is finished)
     uint32_t* h_ids = nullptr;
     int32_t* h_dists = nullptr;
     pgb_query_stats* h_stats = nullptr;
+    uint32_t* h_done = nullptr;
+    uint32_t seq = 0;                   // this context's launch count
+    std::vector<uint32_t> unpublished;  // batch positions not yet handed to their slots
     uint8_t* d_in = nullptr;
     uint32_t* d_ids = nullptr;
     int32_t* d_dists = nullptr;
     pgb_query_stats* d_stats = nullptr;
+    uint32_t* d_done = nullptr;
     uint32_t* d_queue = nullptr;
     uint32_t* gfilter = nullptr;
     uint32_t* gvisited = nullptr;
@@ -116,10 +125,8 @@ void free_context(Context& c) {
     cudaFreeHost(c.h_ids);
     cudaFreeHost(c.h_dists);
     cudaFreeHost(c.h_stats);
+    cudaFreeHost(c.h_done);
     cudaFree(c.d_in);
-    cudaFree(c.d_ids);
-    cudaFree(c.d_dists);
-    cudaFree(c.d_stats);
     cudaFree(c.d_queue);
     cudaFree(c.gfilter);
     cudaFree(c.gvisited);
@@ -146,12 +153,15 @@ pgb_status alloc_context(pgb_server* S, Context& c) {
         (s = cuda_status(cudaMallocHost(&c.h_ids, 4 * mb * mk), "pinned staging")) != PGB_OK ||
         (s = cuda_status(cudaMallocHost(&c.h_dists, 4 * mb * mk), "pinned staging")) != PGB_OK ||
         (s = cuda_status(cudaMallocHost(&c.h_stats, sizeof(pgb_query_stats) * mb), "pinned staging")) != PGB_OK ||
+        (s = cuda_status(cudaMallocHost(&c.h_done, 4 * mb), "pinned flags")) != PGB_OK ||
+        (s = cuda_status(cudaHostGetDevicePointer((void**)&c.d_ids, c.h_ids, 0), "mapped outputs")) != PGB_OK ||
+        (s = cuda_status(cudaHostGetDevicePointer((void**)&c.d_dists, c.h_dists, 0), "mapped outputs")) != PGB_OK ||
+        (s = cuda_status(cudaHostGetDevicePointer((void**)&c.d_stats, c.h_stats, 0), "mapped outputs")) != PGB_OK ||
+        (s = cuda_status(cudaHostGetDevicePointer((void**)&c.d_done, c.h_done, 0), "mapped flags")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&c.d_in, S->in_bytes), "device staging")) != PGB_OK ||
-        (s = cuda_status(cudaMalloc(&c.d_ids, 4 * mb * mk), "device outputs")) != PGB_OK ||
-        (s = cuda_status(cudaMalloc(&c.d_dists, 4 * mb * mk), "device outputs")) != PGB_OK ||
-        (s = cuda_status(cudaMalloc(&c.d_stats, sizeof(pgb_query_stats) * mb), "device outputs")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&c.d_queue, 4), "queue counter")) != PGB_OK)
         return s;
+    memset(c.h_done, 0, 4 * mb);
     if (S->hnsw) {
         const pgb_query_params p = hnsw_params(S);
         return hnsw_prepare(S->index, p, c.hnsw);
@@ -167,8 +177,8 @@ pgb_status alloc_context(pgb_server* S, Context& c) {
 }
 
 size_t context_device_bytes(const pgb_server* S) {
-    const size_t mb = S->opt.max_batch, mk = S->opt.max_k, tw = S->plan.total_warps;
-    const size_t staging = S->in_bytes + 8 * mb * mk + sizeof(pgb_query_stats) * mb + 4;
+    const size_t tw = S->plan.total_warps;
+    const size_t staging = S->in_bytes + 4;  // the outputs live in page-locked host memory
     if (S->hnsw) return staging + S->hnsw_scratch;
     return staging + 4ull * (S->plan.gfilter_words + S->plan.gvisited_words) * tw;
 }
@@ -187,16 +197,12 @@ void fail_unlocked(pgb_server* S, pgb_status s, const std::string& m) {
     set_failed(S, s, m);
 }
 
-// downloads a launched batch's outputs and records its completion event
+// records a launched batch's completion event (its outputs reach host memory from the
+// kernel itself) and lists its positions as unpublished
 bool download(pgb_server* S, Context& c, uint32_t b) {
-    const size_t mk = S->opt.max_k;
-    cudaError_t e = cudaMemcpyAsync(c.h_ids, c.d_ids, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(c.h_dists, c.d_dists, 4ull * b * mk, cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(c.h_stats, c.d_stats, sizeof(pgb_query_stats) * b,
-                            cudaMemcpyDeviceToHost, c.stream);
-    if (e == cudaSuccess) e = cudaEventRecord(c.done, c.stream);
+    c.unpublished.resize(b);
+    std::iota(c.unpublished.begin(), c.unpublished.end(), 0u);
+    cudaError_t e = cudaEventRecord(c.done, c.stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         fail_unlocked(S, PGB_ERR_CUDA, std::string("server launch: ") + cudaGetErrorString(e));
@@ -230,11 +236,15 @@ bool launch(pgb_server* S, Context& c) {
         return false;
     }
     const uint32_t* d_ls = reinterpret_cast<const uint32_t*>(c.d_in + S->in_q_bytes);
+    if (++c.seq == 0) {  // flags of earlier launches hold older values; 0 is never one
+        memset(c.h_done, 0, 4 * mb);
+        c.seq = 1;
+    }
     if (S->hnsw) {
         // one launch of the HNSW kernel: each query at its own (Ls, k), longest beam first
         if (hnsw_launch_at(ix, c.hnsw, S->opt.max_beam, S->opt.max_k, S->opt.limit, c.d_in, b, ix->dim,
                            c.d_ids, c.d_dists, c.d_stats, S->opt.max_k, c.stream, d_ls, d_ls + mb,
-                           d_ls + 2 * mb) != PGB_OK) {
+                           d_ls + 2 * mb, c.d_done, c.seq) != PGB_OK) {
             fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
             return false;
         }
@@ -266,6 +276,8 @@ bool launch(pgb_server* S, Context& c) {
     A.gfilter = c.gfilter;
     A.gvisited = c.gvisited;
     A.queue = c.d_queue;
+    A.done = c.d_done;
+    A.done_seq = c.seq;
     if (launch_flat(S->plan, A, c.stream, ix) != PGB_OK) {
         fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
         return false;
@@ -273,27 +285,60 @@ bool launch(pgb_server* S, Context& c) {
     return download(S, c, b);
 }
 
-// publishes a finished launch: results into the slots (no lock), then counters
-void finish(pgb_server* S, Context& c, std::vector<float>& lat) {
+// hands batch position j's results to its slot (no lock: the slot is this launch's)
+void publish(pgb_server* S, Context& c, uint32_t j, Clock::time_point now, std::vector<float>& lat) {
     const size_t mk = S->opt.max_k;
-    const auto now = Clock::now();
-    lat.clear();
-    for (size_t j = 0; j < c.slots.size(); j++) {
-        Slot& sl = S->pool[c.slots[j]];
-        std::copy(c.h_ids + j * mk, c.h_ids + j * mk + sl.k, sl.ids.begin());
-        std::copy(c.h_dists + j * mk, c.h_dists + j * mk + sl.k, sl.dists.begin());
-        sl.stats = c.h_stats[j];
-        lat.push_back(std::chrono::duration<float, std::micro>(now - sl.t_submit).count());
-        sl.done.store(true, std::memory_order_release);
+    Slot& sl = S->pool[c.slots[j]];
+    std::copy(c.h_ids + j * mk, c.h_ids + j * mk + sl.k, sl.ids.begin());
+    std::copy(c.h_dists + j * mk, c.h_dists + j * mk + sl.k, sl.dists.begin());
+    sl.stats = c.h_stats[j];
+    lat.push_back(std::chrono::duration<float, std::micro>(now - sl.t_submit).count());
+    sl.done.store(true, std::memory_order_release);
+}
+
+void record_latencies(pgb_server* S, const std::vector<float>& lat) {
+    for (float us : lat) {
+        S->lat_us[S->lat_pos] = us;
+        S->lat_pos = (S->lat_pos + 1) % kLatencyRing;
+        if (S->lat_pos == 0) S->lat_full = true;
     }
+    S->completed += lat.size();
+}
+
+// publishes the positions of a running launch whose completion flags are set; returns
+// whether any was
+bool publish_ready(pgb_server* S, Context& c, std::vector<float>& lat) {
+    lat.clear();
+    const auto now = Clock::now();
+    size_t keep = 0;
+    for (size_t i = 0; i < c.unpublished.size(); i++) {
+        const uint32_t j = c.unpublished[i];
+        if (reinterpret_cast<volatile uint32_t*>(c.h_done)[j] == c.seq) {
+            std::atomic_thread_fence(std::memory_order_acquire);  // flag, then its outputs
+            publish(S, c, j, now, lat);
+        } else {
+            c.unpublished[keep++] = j;
+        }
+    }
+    c.unpublished.resize(keep);
+    if (lat.empty()) return false;
     {
         std::lock_guard<std::mutex> lk(S->mu);
-        for (float us : lat) {
-            S->lat_us[S->lat_pos] = us;
-            S->lat_pos = (S->lat_pos + 1) % kLatencyRing;
-            if (S->lat_pos == 0) S->lat_full = true;
-        }
-        S->completed += lat.size();
+        record_latencies(S, lat);
+    }
+    S->cv_done.notify_all();
+    return true;
+}
+
+// a finished launch: the positions not published yet, then the context is free again
+void finish(pgb_server* S, Context& c, std::vector<float>& lat) {
+    const auto now = Clock::now();
+    lat.clear();
+    for (const uint32_t j : c.unpublished) publish(S, c, j, now, lat);
+    c.unpublished.clear();
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        record_latencies(S, lat);
         c.slots.clear();
         c.busy = false;
     }
@@ -308,6 +353,7 @@ void dispatch_loop(pgb_server* S) {
         int inflight = 0;
         for (Context& c : S->ctx) {
             if (!c.busy) continue;  // only this thread changes busy
+            if (publish_ready(S, c, lat)) progressed = true;
             const cudaError_t q = cudaEventQuery(c.done);
             if (q == cudaSuccess) {
                 finish(S, c, lat);
