@@ -838,44 +838,8 @@ pgb_status hnsw_launch_at(const pgb_index* ix, HnswState& H, uint32_t Ls, uint32
         if (s != PGB_OK) return s;
     }
     void* args[] = {&A};
-#ifdef PGB_HNSW_PERSIST_FILTER
-    cudaError_t e;
-    if (H.fmode == 1) {
-        // experiment: the global filter tables as a persisting L2 window
-        static bool limit_set = false;
-        int dev = 0, maxw = 0, maxp = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev);
-        cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev);
-        const size_t tb = 4ull * H.filter_slots * H.total_warps;
-        const size_t win = std::min<size_t>(tb, (size_t)maxw);
-        if (!limit_set) {
-            cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, std::min<size_t>(win, (size_t)maxp));
-            limit_set = true;
-        }
-        cudaLaunchConfig_t cfg{};
-        cfg.gridDim = dim3(H.blocks);
-        cfg.blockDim = dim3(H.warps_per_block * 32);
-        cfg.dynamicSmemBytes = H.smem_bytes;
-        cfg.stream = stream;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeAccessPolicyWindow;
-        at[0].val.accessPolicyWindow.base_ptr = H.gfilter;
-        at[0].val.accessPolicyWindow.num_bytes = win;
-        at[0].val.accessPolicyWindow.hitRatio = std::min(1.0f, (float)maxp / (float)win);
-        at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-        at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        e = cudaLaunchKernelExC(&cfg, H.kernel, args);
-    } else {
-        e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
-                             H.smem_bytes, stream);
-    }
-#else
     cudaError_t e = cudaLaunchKernel(H.kernel, dim3(H.blocks), dim3(H.warps_per_block * 32), args,
                                      H.smem_bytes, stream);
-#endif
     if (e == cudaSuccess) count_launches(1);
     if (e == cudaSuccess && H.d_epoch) {
         hnsw_epoch_advance<<<1, 1, 0, stream>>>(H.d_epoch, need);
