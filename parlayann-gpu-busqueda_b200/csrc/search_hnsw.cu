@@ -39,6 +39,18 @@
 #ifndef PGB_HNSW_SHARED_FILTER_BYTES
 #define PGB_HNSW_SHARED_FILTER_BYTES 4096
 #endif
+// resident 128-thread blocks per SM the HNSW kernel is compiled for (8: 64 registers)
+#ifndef PGB_HNSW_MIN_BLOCKS
+#define PGB_HNSW_MIN_BLOCKS 8
+#endif
+// distance rounds of the HNSW kernel: 8 * slots rows in flight per warp; TAIL: a tail of
+// at most 8 rows takes a one-slot round
+#ifndef PGB_HNSW_DIST_SLOTS
+#define PGB_HNSW_DIST_SLOTS 2
+#endif
+#ifndef PGB_HNSW_DIST_TAIL
+#define PGB_HNSW_DIST_TAIL false
+#endif
 
 namespace pgb {
 
@@ -176,7 +188,7 @@ static __device__ unsigned long long g_hnsw_section_cycles[NUM_SECTIONS];
 // unwritten slots need no load). 2: per-warp global table of (epoch, id) pairs, for
 // filters whose written-bitmap would not fit in shared memory.
 template <int CH, bool Signed, int FMODE>
-__global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
+__global__ void __launch_bounds__(128, PGB_HNSW_MIN_BLOCKS) hnsw_kernel(HnswArgs A) {
     constexpr bool SFILT = FMODE == 0;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31;
@@ -436,7 +448,8 @@ __global__ void __launch_bounds__(128, 8) hnsw_kernel(HnswArgs A) {
                 comps += np;
                 PGB_PROF_COUNT_N(SEC_N_PENDING, np);
                 PGB_PROF_ADD(SEC_FILTER, tp);
-                row_distances<Signed>(A.rows, pend, pd, np, q4, qq, A.dim, A.norm_in_row != 0, lane);
+                row_distances<Signed, PGB_HNSW_DIST_SLOTS, PGB_HNSW_DIST_TAIL>(A.rows, pend, pd, np, q4, qq, A.dim,
+                                                                            A.norm_in_row != 0, lane);
                 PGB_PROF_ADD(SEC_DIST, tp);
 
                 // ---- eligibility (first copy in this expansion, not in is_inw) and
