@@ -199,7 +199,7 @@ void fail_unlocked(pgb_server* S, pgb_status s, const std::string& m) {
 
 // records a launched batch's completion event (its outputs reach host memory from the
 // kernel itself) and lists its positions as unpublished
-bool download(pgb_server* S, Context& c, uint32_t b) {
+bool track_completion(pgb_server* S, Context& c, uint32_t b) {
     c.unpublished.resize(b);
     std::iota(c.unpublished.begin(), c.unpublished.end(), 0u);
     cudaError_t e = cudaEventRecord(c.done, c.stream);
@@ -248,7 +248,7 @@ bool launch(pgb_server* S, Context& c) {
             fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
             return false;
         }
-        return download(S, c, b);
+        return track_completion(S, c, b);
     }
     FlatArgs A{};
     A.rows = ix->rows;
@@ -282,7 +282,7 @@ bool launch(pgb_server* S, Context& c) {
         fail_unlocked(S, PGB_ERR_CUDA, pgb_last_error());
         return false;
     }
-    return download(S, c, b);
+    return track_completion(S, c, b);
 }
 
 // hands batch position j's results to its slot (no lock: the slot is this launch's)
