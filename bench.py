@@ -418,8 +418,9 @@ def run_extras(args, pgb, torch, dev, local, base, queries, graph, gt_ids, gt_d,
     PARITY_SAMPLE queries -- Vamana at the smallest, the operating, the widest swept beam and
     at 316 (global filter and visited tables), and HCNNG, PyNNDescent and HNSW at their own
     recall@10 >= 0.90 beams; (2) those families' plain and batched QPS with the L2 flushed
-    and their gather roofline; (3) the serving loop on the Vamana graph and the HNSW model
-    at two offered rates. Returns the three blocks of the bench line."""
+    and their gather roofline; (3) 100k queries of uneven beams and k in one batched launch
+    against the plain kernel once per (Ls, k), on the Vamana graph and the HNSW model; (4)
+    the serving loop on both at two offered rates. Returns the blocks of the bench line."""
     from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
     t_start = time.time()
     stream = torch.cuda.current_stream(dev)
@@ -505,6 +506,19 @@ def run_extras(args, pgb, torch, dev, local, base, queries, graph, gt_ids, gt_d,
         b.close()
         index.close()
 
+    # the batched form's own case: 100k queries of uneven beams and k in one launch
+    mixed = {}
+    mq = rank_queries(0, MIXED_NQ)
+    for kind in ("vamana", "hnsw"):
+        if kind == "hnsw":
+            _, h = load_hnsw(pgb)
+            index = pgb.Index.hnsw(base, h, device=local)
+        else:
+            index = pgb.Index.flat(base, graph, device=local)
+        mixed[kind] = mixed_leg(pgb, torch, dev, index, mq, 3)
+        log("mixed", kind, {k: v for k, v in mixed[kind].items() if k != "batched_config"})
+        index.close()
+
     serving = {}
     rng = np.random.default_rng(1)
     seconds = float(os.environ.get("PGB_SERVE_SECONDS", "2"))
@@ -519,7 +533,8 @@ def run_extras(args, pgb, torch, dev, local, base, queries, graph, gt_ids, gt_d,
         log("serving", kind, serving[kind])
         index.close()
     log(f"extras in {time.time() - t_start:.1f} s")
-    return {"identical_to_oracle": ident, "families": families, "serving": serving}
+    return {"identical_to_oracle": ident, "families": families, "mixed": mixed,
+            "serving": serving}
 
 
 def gather_rate(pgb, torch, dev, index, query_dev, lanes, count, steps, warmup, flush,
@@ -866,6 +881,7 @@ def main():
         if extras:
             line["config"]["identical_to_oracle"] = extras["identical_to_oracle"]
             line["families"] = extras["families"]
+            line["mixed"] = extras["mixed"]
             line["serving"] = extras["serving"]
         print(json.dumps(line), flush=True)
     plain.liberar()
@@ -1215,37 +1231,26 @@ def run_c4(args, local):
         "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
 
 
-def run_mixed(args, local, kind="vamana"):
-    """100,000 queries with Ls log-uniform in [10, 500] and k in {10, 50, 100}: one batched
-    launch (a CUDA graph) against the plain kernel launched once per distinct (Ls, k);
-    kind "hnsw": the same on the HNSW model (its beams above 256 use the (epoch, id) filter,
-    whose epochs come from a device word, so the graph replays with fresh ones)."""
-    import torch
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    pgb = ge.load_package()
-    nq = 100_000
-    if kind == "hnsw":
-        base, h = load_hnsw(pgb)
-        queries = rank_queries(0, nq)
-        index = pgb.Index.hnsw(base, h, device=local)
-    else:
-        base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana", nq)
-        index = pgb.Index.flat(base, graph, device=local)
+MIXED_NQ = 100_000
+
+
+def mixed_leg(pgb, torch, dev, index, queries, steps):
+    """100,000 queries with Ls log-uniform in [10, 500] and k in {10, 50, 100} (seed 0): one
+    batched launch (tuned, a CUDA graph) against the plain kernel launched once per distinct
+    (Ls, k), the query-index exclusion off in both arms (the plain arm regroups queries).
+    Returns the row of the bench line."""
+    nq = len(queries)
     rng = np.random.default_rng(0)
     ls = np.rint(np.exp(rng.uniform(np.log(10), np.log(500), nq))).astype(np.uint32)
     ks = rng.choice(np.array([10, 50, 100], np.uint32), nq)
-    max_k = 100
     q = torch.from_numpy(queries.view(np.uint8)).to(dev)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
-    # the plain arm regroups queries, so the query-index exclusion is off in both arms
-    b = pgb.Batch(index, nq, max_beam=int(ls.max()), max_k=max_k, exclude_query_id=False)
+    b = pgb.Batch(index, nq, max_beam=int(ls.max()), max_k=100, exclude_query_id=False)
     b.plan(ls, ks)
     ids, d, st = b.outputs(dev)
     tuned = b.tune(q, ids, d, st)
     flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
-    steps = max(3, args.steps // 20)
     b.capture(q, ids, d, st)
     tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, 2, flush)
     # plain: the drop-in prepares one searcher per distinct (Ls, k) and launches it on
@@ -1266,21 +1271,41 @@ def run_mixed(args, local, kind="vamana"):
                                         1, 1))
         same = same and np.array_equal(oi.cpu().numpy().view(np.uint32), got[idx, :k])
         s.liberar()
+    b.close()
     qb = nq * len(tb) / (sum(tb) / 1e3)
     qp = nq / (t_plain_ms / 1e3)
-    plain = list(groups)
+    return {"batched_qps": qb, "plain_qps": qp, "plain_launches_per_step": len(groups),
+            "batched_over_plain": qb / qp, "batched_ms": sum(tb) / len(tb),
+            "plain_timing": "sum of per-group launch times (events), L2 warm",
+            "identical_neighbours": bool(same), "batched_config": tuned,
+            "l2": "flushed before every timed batched step"}
+
+
+def run_mixed(args, local, kind="vamana"):
+    """The mixed-beam batch (mixed_leg) on the Vamana graph, or (kind "hnsw") on the HNSW
+    model (its beams above 256 use the (epoch, id) filter, whose epochs come from a device
+    word, so the graph replays with fresh ones)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    if kind == "hnsw":
+        base, h = load_hnsw(pgb)
+        queries = rank_queries(0, MIXED_NQ)
+        index = pgb.Index.hnsw(base, h, device=local)
+    else:
+        base, queries, graph = load_workload(pgb, 0, lambda: None, "vamana", MIXED_NQ)
+        index = pgb.Index.flat(base, graph, device=local)
+    steps = max(3, args.steps // 20)
+    row = mixed_leg(pgb, torch, dev, index, queries, steps)
     print(json.dumps({
-        "metric": "QPS, 100k queries of uneven Ls and k, batched (one launch) vs plain", "value": qb,
-        "unit": "queries/s", "n_gpus": 1, "steps": steps, "warmup": 2,
-        "ms_per_step": sum(tb) / len(tb), "higher_is_better": True, "scaling": "weak",
+        "metric": "QPS, 100k queries of uneven Ls and k, batched (one launch) vs plain",
+        "value": row["batched_qps"], "unit": "queries/s", "n_gpus": 1, "steps": steps, "warmup": 2,
+        "ms_per_step": row["batched_ms"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "int8", "data": "synthetic",
-        "config": {"workload": "1M int8 d=100 %s, 100000 queries, Ls log-uniform [10,500], "
-                               "k in {10,50,100}" % ("HNSW M32 efc128" if kind == "hnsw" else "Vamana R64"),
-                   "batched_qps": qb, "plain_qps": qp,
-                   "plain_launches_per_step": len(plain), "batched_over_plain": qb / qp,
-                   "plain_timing": "sum of per-group launch times (events), L2 warm",
-                   "identical_neighbours": bool(same), "batched_config": tuned,
-                   "l2": "flushed before every timed step"},
+        "config": dict({"workload": "1M int8 d=100 %s, 100000 queries, Ls log-uniform [10,500], "
+                                    "k in {10,50,100}" % ("HNSW M32 efc128" if kind == "hnsw"
+                                                          else "Vamana R64")}, **row),
         "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
 
 
