@@ -810,10 +810,14 @@ def main():
         ts = []
         for _ in range(5):
             t = time.perf_counter()
-            oid = oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls, threads=threads)[0]
+            o = oracle.flat_search(base, graph.degrees, graph.edges, qs, K, Ls, threads=threads)
             ts.append(time.perf_counter() - t)
-        assert np.array_equal(oid, p_ids[:sample].cpu().numpy().view(np.uint32)), \
-            "CUDA result differs from the CPU restatement"
+        ps = p_st[:sample].cpu().numpy()
+        assert (np.array_equal(o[0], p_ids[:sample].cpu().numpy().view(np.uint32)) and
+                np.array_equal(o[1], p_d[:sample].cpu().numpy()) and
+                np.array_equal(o[2], ps[:, 0]) and np.array_equal(o[3], ps[:, 1]) and
+                np.array_equal(o[4], ps[:, 2])), \
+            "CUDA result (ids, distances, counts or flags) differs from the CPU restatement"
         # the same restatement on one thread, on the first 1,024 of the sample
         q1 = np.ascontiguousarray(queries[:1024])
         t = time.perf_counter()
