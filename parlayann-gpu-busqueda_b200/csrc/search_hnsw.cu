@@ -308,6 +308,7 @@ __global__ void __launch_bounds__(128, PGB_HNSW_MIN_BLOCKS) hnsw_kernel(HnswArgs
             nC = __shfl_sync(kFull, nC, 0);
             nW = __shfl_sync(kFull, nW, 0);
             __syncwarp();
+            int32_t wlast = key_dist(wkey[nW - 1]);  // W's worst distance, kept in a register
             comps += neps;
             uint32_t inserted = (uint32_t)neps;
             uint64_t cnt = 0;
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(128, PGB_HNSW_MIN_BLOCKS) hnsw_kernel(HnswArgs
 
             PGB_PROF_ADD(SEC_SETUP, tp);
             while (nC > 0) {
-                if (key_dist(ckey[c0]) > key_dist(wkey[nW - 1])) break;
+                if (key_dist(ckey[c0]) > wlast) break;
                 if (++cnt > limit) break;
                 const uint32_t u = key_id(ckey[c0]);
                 c0++;  // pop the closest candidate
@@ -459,31 +460,36 @@ __global__ void __launch_bounds__(128, PGB_HNSW_MIN_BLOCKS) hnsw_kernel(HnswArgs
                 // "near" neighbours are checked at all. Copies of an id share a distance,
                 // so the first copy of a near id is near too.
                 const int m = max(ef, nW);
-                const int32_t worst = nW >= ef ? key_dist(wkey[nW - 1]) : INT_MAX;
+                const int32_t worst = nW >= ef ? wlast : INT_MAX;
                 int na = 0;
                 if (np <= 32) {
                     // one chunk: earlier copies are the lanes below with the same id, and
-                    // the earlier eligible neighbours are a ballot mask
+                    // the earlier eligible neighbours are a ballot mask. Only near lanes
+                    // take part (copies of an id share a distance), and an expansion with
+                    // none (most of them) skips the rest.
                     const uint32_t pv = lane < np ? pend[lane] : kEmptyId;
                     const int32_t dv = lane < np ? pd[lane] : INT_MAX;
-                    const bool first = (__match_any_sync(kFull, pv) & lt) == 0;
-                    bool elig = lane < np && dv < worst && first;
-                    int c = 0;
-                    if (elig) {
-                        bool in_w;
-                        c = w_count_le(wkey, nW, dv, pv, in_w);
-                        elig = !in_w;
+                    const bool near = lane < np && dv < worst;
+                    const uint32_t nm = __ballot_sync(kFull, near);
+                    if (nm) {
+                        bool elig = false;
+                        int c = 0;
+                        if (near && (__match_any_sync(nm, pv) & lt) == 0) {
+                            bool in_w;
+                            c = w_count_le(wkey, nW, dv, pv, in_w);
+                            elig = !in_w;
+                        }
+                        const uint32_t em = __ballot_sync(kFull, elig);
+                        bool acc = false;
+                        if (elig) {
+                            for (uint32_t mm = em & lt; mm != 0u && c < m; mm &= mm - 1u)
+                                c += pd[__ffs(mm) - 1] <= dv ? 1 : 0;
+                            acc = c < m;
+                        }
+                        const uint32_t mk = __ballot_sync(kFull, acc);
+                        if (acc) akey[__popc(mk & lt)] = pack_key(dv, pv);
+                        na = __popc(mk);
                     }
-                    const uint32_t em = __ballot_sync(kFull, elig);
-                    bool acc = false;
-                    if (elig) {
-                        for (uint32_t mm = em & lt; mm != 0u && c < m; mm &= mm - 1u)
-                            c += pd[__ffs(mm) - 1] <= dv ? 1 : 0;
-                        acc = c < m;
-                    }
-                    const uint32_t mk = __ballot_sync(kFull, acc);
-                    if (acc) akey[__popc(mk & lt)] = pack_key(dv, pv);
-                    na = __popc(mk);
                 } else {
                     for (int j = lane; j < np; j += 32) {
                         const uint32_t pv = pend[j];
@@ -625,6 +631,7 @@ __global__ void __launch_bounds__(128, PGB_HNSW_MIN_BLOCKS) hnsw_kernel(HnswArgs
                         if (pos[j] < nWn) wkey[pos[j]] = akey[j];
                     __syncwarp();
                     nW = nWn;
+                    wlast = key_dist(wkey[nW - 1]);
                     PGB_PROF_ADD(SEC_SHIFT, tp);
                 } else if (nC > 0) {
                     request_row(key_id(ckey[c0]));  // cand unchanged
