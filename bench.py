@@ -622,7 +622,7 @@ def main():
                     help="warps per block of the profiled batched launch")
     ap.add_argument("--workload", default="vamana",
                     choices=["vamana", "hcnng", "nnd", "hnsw", "mixed", "mixed_hnsw", "serving",
-                             "serving_hnsw", "c4", "build", "codes", "gather"],
+                             "serving_hnsw", "c4", "build", "codes", "gather", "sweep"],
                     help="vamana (default, the headline): plain vs batched at recall 0.90; "
                          "hcnng / nnd: the same on the other flat graphs; hnsw: HNSW search; "
                          "mixed / mixed_hnsw: 100k queries of uneven Ls and k in one launch "
@@ -631,7 +631,8 @@ def main():
                          "graph / the HNSW model; c4: 10M uint8 d=128 Vamana, 100k queries, "
                          "Ls 20/50/100/200; build: GPU vs CPU Vamana, HNSW and HCNNG "
                          "construction on the 1M base; codes: 4-bit code rows + exact re-rank "
-                         "vs vector rows, plain kernel, 1M Vamana")
+                         "vs vector rows, plain kernel, 1M Vamana; sweep: every family at "
+                         "every sweep beam, plain and batched, against the oracle")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if args.prepare:
@@ -644,11 +645,12 @@ def main():
             run_profile(args, local)
         return
     if args.workload in ("hnsw", "mixed", "mixed_hnsw", "serving", "serving_hnsw", "c4",
-                         "build", "codes", "gather") and args.impl == "ours":
+                         "build", "codes", "gather", "sweep") and args.impl == "ours":
         {"hnsw": run_hnsw, "mixed": run_mixed, "mixed_hnsw": lambda a, lo: run_mixed(a, lo, "hnsw"),
          "serving": run_serving,
          "serving_hnsw": lambda a, lo: run_serving(a, lo, "hnsw"), "c4": run_c4,
-         "build": run_build, "codes": run_codes, "gather": run_gather}[args.workload](args, local)
+         "build": run_build, "codes": run_codes, "gather": run_gather,
+         "sweep": run_sweep}[args.workload](args, local)
         return
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -973,6 +975,97 @@ def run_hnsw(args, local):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "peak_source": kind,
                      "kernel": "hnsw_kernel"},
+        "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
+
+
+SWEEP_SAMPLE = 256  # queries of each sweep configuration checked against the oracle
+
+
+def run_sweep(args, local):
+    """The reference's full comparison grid (cuda/comparacion1.cu:33-36: every graph family
+    at every beam of the sweep) on the 1M workload: Vamana, HCNNG, PyNNDescent and HNSW at
+    the 18 beams 10..500, k=10, 29,316 queries. Per configuration: recall@10, plain and
+    batched (tuned, captured) QPS with the L2 flushed before every timed step, the batched
+    launch's gather roofline, plain and batched identical on every query, and the first
+    SWEEP_SAMPLE queries identical to the oracle (ids, distances, counts, flags)."""
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pgb = ge.load_package()
+    oracle = ge.load_oracle()
+    from parlayann_gpu_busqueda_b200.synthetic import LS_SWEEP
+    base = load_base(pgb)
+    queries = rank_queries(0)
+    gt_ids, gt_d = ground_truth(base, queries, 0, local)
+    q_dev = torch.from_numpy(queries.view(np.uint8)).to(dev)
+    qs = np.ascontiguousarray(queries[:SWEEP_SAMPLE])
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    flush = torch.empty(512 * 2**20, dtype=torch.uint8, device=dev)
+    peak, kind_peak = measured_peaks()
+    steps, warmup = max(1, min(args.steps, 5)), max(3, min(args.warmup, 3))
+    t_start = time.time()
+    table = {}
+    for kind in ("vamana", "hcnng", "nnd", "hnsw"):
+        if kind == "hnsw":
+            _, fg = load_hnsw(pgb)
+            index = pgb.Index.hnsw(base, fg, device=local)
+        else:
+            _, _, fg = load_workload(pgb, 0, lambda: None, kind)
+            index = pgb.Index.flat(base, fg, device=local)
+        gsz = (int(index.info.max_degree) + 31) // 32 * 32
+        rows = []
+        for ls in LS_SWEEP:
+            plain = pgb.Searcher(index, N_QUERIES, pgb.QueryParams(k=K, beam_size=ls))
+            p_ids = torch.empty((N_QUERIES, K), dtype=torch.int32, device=dev)
+            p_d = torch.empty_like(p_ids)
+            p_st = torch.empty((N_QUERIES, 4), dtype=torch.int32, device=dev)
+            tp = _timed_events(torch, stream, lambda: plain.lanzar(q_dev, p_ids, p_d, p_st, sp),
+                               steps, warmup, flush)
+            b = pgb.Batch(index, N_QUERIES, max_beam=ls, max_k=K)
+            b.plan(np.full(N_QUERIES, ls, np.uint32), np.full(N_QUERIES, K, np.uint32))
+            bi, bd, bs = b.outputs(dev)
+            b.tune(q_dev, bi, bd, bs)
+            b.capture(q_dev, bi, bd, bs)
+            tb = _timed_events(torch, stream, lambda: b.replay(sp), steps, warmup, flush)
+            torch.cuda.synchronize(dev)
+            ids_h = p_ids.cpu().numpy().view(np.uint32)
+            stn = p_st.cpu().numpy()
+            o = (oracle.hnsw_search(base, fg, qs, K, ls) if kind == "hnsw"
+                 else oracle.flat_search(base, fg.degrees, fg.edges, qs, K, ls))
+            same_oracle = bool(np.array_equal(ids_h[:SWEEP_SAMPLE], o[0]) and
+                               np.array_equal(p_d.cpu().numpy()[:SWEEP_SAMPLE], o[1]) and
+                               all(np.array_equal(stn[:SWEEP_SAMPLE, c], o[2 + c]) for c in range(3)))
+            same_forms = bool(torch.equal(p_ids, bi) and torch.equal(p_d, bd) and
+                              torch.equal(p_st[:, :3], bs[:, :3]))
+            mp, mb = sum(tp) / len(tp) / 1e3, sum(tb) / len(tb) / 1e3
+            bytes_launch = float(128 * stn[:, 0].astype(np.int64).sum() +
+                                 4 * gsz * stn[:, 1].astype(np.int64).sum())
+            rows.append({"Ls": ls, "recall_at_10": round(pgb.recall(gt_ids, gt_d, ids_h, K), 5),
+                         "plain_qps": N_QUERIES / mp, "batched_qps": N_QUERIES / mb,
+                         "batched_over_plain": mp / mb, "frac": bytes_launch / mb / 1e9 / peak,
+                         "comps_per_query": float(stn[:, 0].mean()),
+                         "expansions_per_query": float(stn[:, 1].mean()),
+                         "identical_plain_batched": same_forms,
+                         "identical_to_oracle": same_oracle})
+            log(kind, rows[-1])
+            plain.liberar()
+            b.close()
+        table[kind] = rows
+        index.close()
+    print(json.dumps({
+        "metric": "QPS and recall@10 over the beam sweep, plain and batched, 1 B200",
+        "unit": "queries/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
+        "data": "synthetic", "dtype": "int8",
+        "config": {"workload": "1M int8 d=100 Gaussian mixture, 29316 queries, k=10; Vamana R64 "
+                               "L128, HCNNG 30x1000 MST3, PyNNDescent K40, HNSW M32 efc128",
+                   "beams": LS_SWEEP, "l2": "flushed before every timed step",
+                   "oracle_sample": SWEEP_SAMPLE, "peak_gbs": peak, "peak_source": kind_peak},
+        "configurations": sum(len(v) for v in table.values()),
+        "all_identical_to_oracle": all(r["identical_to_oracle"] for v in table.values() for r in v),
+        "all_identical_plain_batched": all(r["identical_plain_batched"] for v in table.values()
+                                           for r in v),
+        "seconds": round(time.time() - t_start, 1), "table": table,
         "gpu_launches": _TIMED_LAUNCHES[0]}), flush=True)
 
 
