@@ -3,9 +3,12 @@
 // plan   : host step, per-query (Ls, k) -> longest-beam-first work order on the device
 // search : cudaMemsetAsync(counter) + one persistent launch (capturable); a plan whose
 //          queries all share one (Ls, k) runs the uniform-batch kernel
-// tune   : times candidate (warps per block, filter / visited placement) on the planned
-//          queries and keeps the fastest; every candidate returns identical neighbours,
-//          because all of them run the same per-query code (flat_query)
+// tune   : times candidate (warps per block, filter / visited placement, resident blocks
+//          per SM) on the planned queries and keeps the fastest; every candidate returns
+//          identical neighbours, because all of them run the same per-query code
+//          (flat_query). Fewer resident warps than fit can win on a batch of a few queries
+//          per warp: the launch ends when its last query does, and with fewer warps each
+//          takes more queries, so the tail in which SMs idle is a smaller share.
 // An HNSW index runs the HNSW kernel with each query at its own (Ls, k), its tables sized
 // for max_beam; it has a single launch shape, so tune only times it. Every beam can be
 // captured: the (epoch, id) filter of beams above 256 takes its epochs from a device word.
@@ -53,7 +56,9 @@ struct pgb_batch {
 namespace pgb {
 namespace {
 
-pgb_status make_plan(pgb_batch* b, int wpb, int filter_pl, int visited_pl, FlatPlan& P) {
+// max_bps: a cap on resident blocks per SM (0: as many as fit)
+pgb_status make_plan(pgb_batch* b, int wpb, int filter_pl, int visited_pl, FlatPlan& P,
+                     int max_bps = 0) {
     const pgb_index* ix = b->index;
     FlatPlanRequest rq;
     rq.max_ls = b->opt.max_beam;
@@ -61,6 +66,7 @@ pgb_status make_plan(pgb_batch* b, int wpb, int filter_pl, int visited_pl, FlatP
     rq.is_signed = ix->elem == PGB_INT8;
     rq.batched = true;
     rq.warps_per_block = wpb;
+    rq.max_blocks_per_sm = max_bps;
     if (filter_pl) {
         rq.force_filter_placement = true;
         rq.filter_in_shared = filter_pl == 1;
@@ -334,23 +340,32 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
                 if (b->opt.warps_per_block && (int)b->opt.warps_per_block != wpb) continue;
                 if (b->opt.filter_placement && (int)b->opt.filter_placement != fp) continue;
                 if (b->opt.visited_placement && (int)b->opt.visited_placement != vp) continue;
-                FlatPlan P;
-                if (make_plan(b, wpb, fp, vp, P) != PGB_OK) continue;  // does not fit
-                if (P.warps_per_block != wpb) continue;
-                if (ensure_scratch(b, P) != PGB_OK) continue;
-                float ms = 0.f, t = 0.f;
-                bool ok = enqueue(b, P, queries, qstride, ids, dists, stats, st) == PGB_OK;  // warm
-                for (int r = 0; r < 2 && ok; r++) {
-                    cudaEventRecord(e0, st);
-                    ok = enqueue(b, P, queries, qstride, ids, dists, stats, st) == PGB_OK;
-                    cudaEventRecord(e1, st);
-                    ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
-                    cudaEventElapsedTime(&t, e0, e1);
-                    ms += t;
-                }
-                if (ok && ms / 2 < best) {
-                    best = ms / 2;
-                    best_plan = P;
+                FlatPlan full;
+                if (make_plan(b, wpb, fp, vp, full) != PGB_OK) continue;  // does not fit
+                if (full.warps_per_block != wpb) continue;
+                // every block that fits, then three quarters and five eighths of them
+                const int caps[] = {0, (3 * full.blocks_per_sm) / 4, (5 * full.blocks_per_sm) / 8};
+                int last = full.blocks_per_sm;
+                for (int cap : caps) {
+                    if (cap != 0 && (cap < 1 || cap >= last)) continue;
+                    FlatPlan P = full;
+                    if (cap != 0 && make_plan(b, wpb, fp, vp, P, cap) != PGB_OK) continue;
+                    last = P.blocks_per_sm;
+                    if (ensure_scratch(b, P) != PGB_OK) continue;
+                    float ms = 0.f, t = 0.f;
+                    bool ok = enqueue(b, P, queries, qstride, ids, dists, stats, st) == PGB_OK;  // warm
+                    for (int r = 0; r < 2 && ok; r++) {
+                        cudaEventRecord(e0, st);
+                        ok = enqueue(b, P, queries, qstride, ids, dists, stats, st) == PGB_OK;
+                        cudaEventRecord(e1, st);
+                        ok = ok && cudaEventSynchronize(e1) == cudaSuccess;
+                        cudaEventElapsedTime(&t, e0, e1);
+                        ms += t;
+                    }
+                    if (ok && ms / 2 < best) {
+                        best = ms / 2;
+                        best_plan = P;
+                    }
                 }
             }
     cudaEventDestroy(e0);
