@@ -282,7 +282,8 @@ pgb_status pgb_batch_search(pgb_batch* b, const void* queries, uint32_t query_st
  * pin_memory), the launch reads and writes them directly and no staging copy is made. */
 pgb_status pgb_batch_search_host(pgb_batch* b, const void* queries, uint32_t query_stride,
                                  uint32_t* ids, int32_t* dists, pgb_query_stats* stats);
-/* Autotuner: times the candidate launch shapes and table placements on the planned
+/* Autotuner: times the candidate launch shapes (warps per block; all resident blocks per
+ * SM, three quarters or five eighths of them) and table placements on the planned
  * queries (outputs are overwritten) and keeps the fastest. Synchronous. */
 pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t query_stride,
                           uint32_t* ids, int32_t* dists, pgb_query_stats* stats);
