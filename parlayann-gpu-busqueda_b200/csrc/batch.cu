@@ -346,10 +346,12 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
                 // every block that fits, then three quarters and five eighths of them
                 const int caps[] = {0, (3 * full.blocks_per_sm) / 4, (5 * full.blocks_per_sm) / 8};
                 int last = full.blocks_per_sm;
-                for (int cap : caps) {
-                    if (cap != 0 && (cap < 1 || cap >= last)) continue;
+                for (int c = 0; c < 3; c++) {
+                    const int cap = caps[c];
+                    // a reduced cap is tried only when it keeps a block and drops one
+                    if (c > 0 && (cap < 1 || cap >= last)) continue;
                     FlatPlan P = full;
-                    if (cap != 0 && make_plan(b, wpb, fp, vp, P, cap) != PGB_OK) continue;
+                    if (c > 0 && make_plan(b, wpb, fp, vp, P, cap) != PGB_OK) continue;
                     last = P.blocks_per_sm;
                     if (ensure_scratch(b, P) != PGB_OK) continue;
                     float ms = 0.f, t = 0.f;
