@@ -260,6 +260,7 @@ typedef struct pgb_batch_options {
     uint32_t warps_per_block;   /* 1, 2 or 4; 0: default (4) / tuned                    */
     uint32_t filter_placement;  /* 0 auto, 1 shared memory (max_beam <= 128), 2 global  */
     uint32_t visited_placement; /* 0 auto, 1 shared memory, 2 global memory             */
+    uint32_t blocks_per_sm;     /* cap on resident blocks per SM; 0: all that fit / tuned */
 } pgb_batch_options;
 
 typedef struct pgb_batch_config {

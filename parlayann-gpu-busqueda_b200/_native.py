@@ -126,7 +126,7 @@ class BatchOptions(C.Structure):
                 ("cut", C.c_double), ("limit", C.c_int64), ("degree_limit", C.c_uint32),
                 ("exclude_query_id", C.c_uint32), ("query_id_base", C.c_uint32),
                 ("warps_per_block", C.c_uint32), ("filter_placement", C.c_uint32),
-                ("visited_placement", C.c_uint32)]
+                ("visited_placement", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
 
 
 class BatchConfig(C.Structure):

@@ -194,7 +194,7 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
     hp.limit = opt->limit;
     if ((s = b->hnsw ? hnsw_prepare(ix, hp, b->hs)
                      : make_plan(b, (int)opt->warps_per_block, (int)opt->filter_placement,
-                                 (int)opt->visited_placement, b->plan)) != PGB_OK ||
+                                 (int)opt->visited_placement, b->plan, (int)opt->blocks_per_sm)) != PGB_OK ||
         (!b->hnsw && (s = ensure_scratch(b, b->plan)) != PGB_OK) ||
         (s = cuda_status(cudaMalloc(&b->d_ls, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_k, 4 * nq), "batch arrays")) != PGB_OK ||
@@ -341,10 +341,12 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
                 if (b->opt.filter_placement && (int)b->opt.filter_placement != fp) continue;
                 if (b->opt.visited_placement && (int)b->opt.visited_placement != vp) continue;
                 FlatPlan full;
-                if (make_plan(b, wpb, fp, vp, full) != PGB_OK) continue;  // does not fit
+                const int fixed = (int)b->opt.blocks_per_sm;  // the caller's cap, if any
+                if (make_plan(b, wpb, fp, vp, full, fixed) != PGB_OK) continue;  // does not fit
                 if (full.warps_per_block != wpb) continue;
                 // every block that fits, then three quarters and five eighths of them
-                const int caps[] = {0, (3 * full.blocks_per_sm) / 4, (5 * full.blocks_per_sm) / 8};
+                const int caps[] = {0, fixed ? 0 : (3 * full.blocks_per_sm) / 4,
+                                    fixed ? 0 : (5 * full.blocks_per_sm) / 8};
                 int last = full.blocks_per_sm;
                 for (int c = 0; c < 3; c++) {
                     const int cap = caps[c];

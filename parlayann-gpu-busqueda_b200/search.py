@@ -339,11 +339,13 @@ class Batch:
     def __init__(self, index: Index, max_queries: int, max_beam: int, max_k: int,
                  cut: float = 1.35, limit: int = 0, degree_limit: int = 0,
                  exclude_query_id: bool = True, query_id_base: int = 0,
-                 warps_per_block: int = 0, filter_placement: int = 0, visited_placement: int = 0):
+                 warps_per_block: int = 0, filter_placement: int = 0, visited_placement: int = 0,
+                 blocks_per_sm: int = 0):
         self.index, self.max_k = index, max_k
         self._opt = N.BatchOptions(max_queries, max_beam, max_k, float(cut), int(limit),
                                    degree_limit, 1 if exclude_query_id else 0, query_id_base,
-                                   warps_per_block, filter_placement, visited_placement)
+                                   warps_per_block, filter_placement, visited_placement,
+                                   blocks_per_sm)
         h = C.c_void_p()
         N.check(N.lib.pgb_batch_create(index.handle, C.byref(self._opt), C.byref(h)))
         self._h = h

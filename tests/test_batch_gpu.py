@@ -88,6 +88,35 @@ def test_batch_placements_identical(pgb, golden, gpu, placement):
     assert_same("dists", dists.cpu().numpy(), want_d)
 
 
+@pytest.mark.parametrize("blocks_per_sm", [1, 3, 0])
+def test_batch_resident_block_cap_identical(pgb, golden, gpu, blocks_per_sm):
+    """A cap on resident blocks per SM (a tuner candidate, or the caller's option) only
+    changes how many warps share the queue: the neighbours are the plain search's, and
+    tune() with a fixed cap keeps it."""
+    import torch
+    base, queries = golden.vectors_for("vamana")
+    index = pgb.Index.flat(base, golden.graphs["vamana"])
+    nq = len(queries)
+    want_i, want_d, want_s = pgb.Searcher(index, nq, pgb.QueryParams(k=10, beam_size=40)).search(queries)
+    b = pgb.Batch(index, nq, max_beam=40, max_k=10, blocks_per_sm=blocks_per_sm)
+    b.plan(np.full(nq, 40), np.full(nq, 10))
+    q = torch.from_numpy(queries.view(np.uint8)).cuda()
+    ids, dists, stats = b.outputs(q.device)
+    b.tune(q, ids, dists, stats)
+    cfg = b.config()
+    if blocks_per_sm:
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        assert cfg["blocks"] == blocks_per_sm * sms, cfg
+    ids.fill_(0)
+    b.search(q, ids, dists, stats)
+    torch.cuda.synchronize()
+    assert_same("ids", ids.cpu().numpy().view(np.uint32), want_i)
+    assert_same("dists", dists.cpu().numpy(), want_d)
+    assert_same("stats", stats.cpu().numpy()[:, :3], want_s[:, :3])
+    b.close()
+    index.close()
+
+
 def test_batch_uniform_and_per_query_kernels_agree(pgb, golden, gpu):
     """A plan whose queries share one (Ls, k) runs the uniform-batch kernel; changing one
     query's beam switches to the per-query kernel. Both give the plain search's output."""
