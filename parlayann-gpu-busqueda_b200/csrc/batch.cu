@@ -10,7 +10,7 @@
 //          per warp: the launch ends when its last query does, and with fewer warps each
 //          takes more queries, so the tail in which SMs idle is a smaller share.
 // An HNSW index runs the HNSW kernel with each query at its own (Ls, k), its tables sized
-// for max_beam; it has a single launch shape, so tune only times it. Every beam can be
+// for max_beam; its one kernel shape is tuned over resident blocks only. Every beam can be
 // captured: the (epoch, id) filter of beams above 256 takes its epochs from a device word.
 #include <algorithm>
 #include <numeric>
@@ -97,6 +97,15 @@ pgb_status ensure_scratch(pgb_batch* b, const FlatPlan& P) {
         if ((s = cuda_status(cudaMalloc(&b->gvisited, 4 * vw), "batch visited scratch")) != PGB_OK) return s;
         b->gvisited_words = vw;
     }
+    return PGB_OK;
+}
+
+// an HNSW batch launches at most max_bps blocks per SM (its tables stay sized for all)
+pgb_status cap_hnsw_blocks(pgb_batch* b, int max_bps) {
+    int sms = 1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->index->device) != cudaSuccess)
+        return cuda_status(cudaGetLastError(), "device attribute");
+    b->hs.blocks = std::min(b->hs.blocks, max_bps * sms);
     return PGB_OK;
 }
 
@@ -196,6 +205,7 @@ pgb_status pgb_batch_create(pgb_index* ix, const pgb_batch_options* opt, pgb_bat
                      : make_plan(b, (int)opt->warps_per_block, (int)opt->filter_placement,
                                  (int)opt->visited_placement, b->plan, (int)opt->blocks_per_sm)) != PGB_OK ||
         (!b->hnsw && (s = ensure_scratch(b, b->plan)) != PGB_OK) ||
+        (b->hnsw && opt->blocks_per_sm && (s = cap_hnsw_blocks(b, (int)opt->blocks_per_sm)) != PGB_OK) ||
         (s = cuda_status(cudaMalloc(&b->d_ls, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_k, 4 * nq), "batch arrays")) != PGB_OK ||
         (s = cuda_status(cudaMalloc(&b->d_order, 4 * nq), "batch arrays")) != PGB_OK ||
@@ -308,25 +318,47 @@ pgb_status pgb_batch_tune(pgb_batch* b, const void* queries, uint32_t qstride, u
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     if (b->hnsw) {
-        // one launch shape: time it (warm-up, then the mean of two)
-        float ms = 0.f, t = 0.f;
-        s = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
-        for (int r = 0; r < 2 && s == PGB_OK; r++) {
-            cudaEventRecord(e0, st);
-            s = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
-            cudaEventRecord(e1, st);
-            if (s == PGB_OK && cudaEventSynchronize(e1) == cudaSuccess) {
-                cudaEventElapsedTime(&t, e0, e1);
-                ms += t;
+        // one kernel shape; the resident blocks are all that fit, three quarters or five
+        // eighths of them (fewer warps also hold fewer global filter tables in L2). The
+        // tables stay allocated for every warp of the prepared shape, so an epoch
+        // wrap-around still clears all of them.
+        int sms = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->index->device);
+        const int full = b->hs.blocks, bps = std::max(1, full / std::max(1, sms));
+        const bool fixed = b->opt.blocks_per_sm != 0;
+        const int cands[] = {full, fixed ? 0 : (3 * bps / 4) * sms, fixed ? 0 : (5 * bps / 8) * sms};
+        float best = 1e30f;
+        int best_blocks = full, last = full + 1;
+        for (int c = 0; c < 3 && s == PGB_OK; c++) {
+            const int blocks = cands[c];
+            if (blocks < sms || blocks >= last) continue;
+            last = blocks;
+            b->hs.blocks = blocks;
+            float ms = 0.f, t = 0.f;
+            s = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);  // warm
+            for (int r = 0; r < 2 && s == PGB_OK; r++) {
+                cudaEventRecord(e0, st);
+                s = enqueue(b, b->plan, queries, qstride, ids, dists, stats, st);
+                cudaEventRecord(e1, st);
+                if (s == PGB_OK && cudaEventSynchronize(e1) == cudaSuccess) {
+                    cudaEventElapsedTime(&t, e0, e1);
+                    ms += t;
+                }
+            }
+            if (s == PGB_OK && ms / 2 < best) {
+                best = ms / 2;
+                best_blocks = blocks;
             }
         }
+        b->hs.blocks = best_blocks;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         const cudaError_t e = cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
         if (s != PGB_OK) return s;
         if (e != cudaSuccess) return cuda_status(e, "tune");
-        b->tuned_ms = ms / 2;
+        b->tuned_ms = best;
+        drop_graph(b);
         return PGB_OK;
     }
     const int wpbs[] = {1, 2, 4};

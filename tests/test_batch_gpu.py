@@ -88,14 +88,16 @@ def test_batch_placements_identical(pgb, golden, gpu, placement):
     assert_same("dists", dists.cpu().numpy(), want_d)
 
 
+@pytest.mark.parametrize("kind", ["vamana", "hnsw"])
 @pytest.mark.parametrize("blocks_per_sm", [1, 3, 0])
-def test_batch_resident_block_cap_identical(pgb, golden, gpu, blocks_per_sm):
+def test_batch_resident_block_cap_identical(pgb, golden, gpu, kind, blocks_per_sm):
     """A cap on resident blocks per SM (a tuner candidate, or the caller's option) only
     changes how many warps share the queue: the neighbours are the plain search's, and
     tune() with a fixed cap keeps it."""
     import torch
-    base, queries = golden.vectors_for("vamana")
-    index = pgb.Index.flat(base, golden.graphs["vamana"])
+    base, queries = golden.vectors_for(kind)
+    index = (pgb.Index.hnsw(base, golden.hnsw[kind]) if kind == "hnsw"
+             else pgb.Index.flat(base, golden.graphs[kind]))
     nq = len(queries)
     want_i, want_d, want_s = pgb.Searcher(index, nq, pgb.QueryParams(k=10, beam_size=40)).search(queries)
     b = pgb.Batch(index, nq, max_beam=40, max_k=10, blocks_per_sm=blocks_per_sm)
