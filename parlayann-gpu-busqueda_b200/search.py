@@ -334,7 +334,9 @@ class Batch:
 
     plan() is the host step (longest beam first work order); search()/replay() are
     device-only and return the same neighbours as Searcher with the same params.
-    Output rows have stride max_k."""
+    Output rows have stride max_k. warps_per_block, filter_placement,
+    visited_placement and blocks_per_sm (a cap on resident blocks per SM) fix parts of
+    the launch shape (0: automatic); tune() times the rest on the planned queries."""
 
     def __init__(self, index: Index, max_queries: int, max_beam: int, max_k: int,
                  cut: float = 1.35, limit: int = 0, degree_limit: int = 0,
